@@ -517,10 +517,85 @@ namespace oracle
   }
 
   // ----------------------------------------------------------------- Vanka
+  namespace
+  {
+    // LU with partial pivoting followed by inversion from the factors, in
+    // working precision T (the LAPACK getrf/getri path that
+    // FullMatrix::gauss_jordan takes for matrices larger than 15x15).
+    template <typename T>
+    void
+    lu_invert(std::vector<T> &A, int n)
+    {
+      auto             at = [&](int i, int j) -> T & { return A[std::size_t(i) * n + j]; };
+      std::vector<int> piv(n);
+      for (int k = 0; k < n; ++k)
+        {
+          int r = k;
+          for (int i = k + 1; i < n; ++i)
+            if (std::abs(at(i, k)) > std::abs(at(r, k)))
+              r = i;
+          piv[k] = r;
+          if (at(r, k) == T(0))
+            throw std::runtime_error("lu_invert: singular");
+          if (r != k)
+            for (int j = 0; j < n; ++j)
+              std::swap(at(k, j), at(r, j));
+          const T d = T(1) / at(k, k);
+          for (int i = k + 1; i < n; ++i)
+            {
+              at(i, k) *= d;
+              const T l = at(i, k);
+              for (int j = k + 1; j < n; ++j)
+                at(i, j) -= l * at(k, j);
+            }
+        }
+      // inv(U) in place (upper triangle)
+      for (int j = 0; j < n; ++j)
+        {
+          at(j, j) = T(1) / at(j, j);
+          const T ajj = -at(j, j);
+          for (int i = 0; i < j; ++i)
+            {
+              T s = 0;
+              for (int k = i; k < j; ++k)
+                s += at(i, k) * at(k, j);
+              at(i, j) = s * ajj;
+            }
+        }
+      // solve inv(A) L = inv(U) for inv(A), columns right to left
+      std::vector<T> work(n);
+      for (int j = n - 2; j >= 0; --j)
+        {
+          for (int i = j + 1; i < n; ++i)
+            {
+              work[i]  = at(i, j);
+              at(i, j) = T(0);
+            }
+          for (int i = 0; i < n; ++i)
+            {
+              T s = 0;
+              for (int k = j + 1; k < n; ++k)
+                s += at(i, k) * work[k];
+              at(i, j) -= s;
+            }
+        }
+      // undo the row interchanges as column interchanges
+      for (int j = n - 2; j >= 0; --j)
+        if (piv[j] != j)
+          for (int i = 0; i < n; ++i)
+            std::swap(at(i, j), at(i, piv[j]));
+    }
+  } // namespace
+
   template <typename T>
   void
   gauss_jordan(std::vector<T> &A, int n)
   {
+    if (n > 15)
+      {
+        lu_invert(A, n);
+        return;
+      }
     std::vector<int> p(n);
     for (int i = 0; i < n; ++i)
       p[i] = i;
