@@ -1,0 +1,67 @@
+// Host object behind stmg_op_t: the space-time operator A (x) K + B (x) M on
+// one mesh level (SystemMatrix, tests/include/operators.h:71-256).
+#pragma once
+
+#include "stmg_internal.h"
+
+namespace stmg
+{
+  class StOperator
+  {
+  public:
+    StOperator(Mesh *mesh, int nt_out, int nt_in, const double *A, const double *B, int dtype);
+
+    // dst (+)= op(src) (transpose: A^T, B^T) on stream s
+    void apply(bool transpose, const void *src, void *dst, bool add, cudaStream_t s) const;
+
+    Mesh               *mesh;
+    int                 nt_out, nt_in, dtype;
+    std::vector<double> A, B;
+    Tiling              tiling, tilingT;
+
+    template <typename T>
+    const TimeMats<T> &tm() const
+    {
+      if constexpr (sizeof(T) == 8)
+        return tm64;
+      else
+        return tm32;
+    }
+    template <typename T>
+    const TimeMats<T> &tmT() const
+    {
+      if constexpr (sizeof(T) == 8)
+        return tmT64;
+      else
+        return tmT32;
+    }
+    template <typename T>
+    const Cart1D<T> &cart() const
+    {
+      if constexpr (sizeof(T) == 8)
+        return cart64;
+      else
+        return cart32;
+    }
+    template <typename T>
+    const QTab<T> &qtab() const
+    {
+      if constexpr (sizeof(T) == 8)
+        return qtab64;
+      else
+        return qtab32;
+    }
+    std::size_t smem_bytes(const Tiling &tl, int nt_in, int nt_out, std::size_t elem) const;
+
+  private:
+    Tiling choose_tiling(int nt_in, int nt_out) const;
+
+    TimeMats<double> tm64, tmT64;
+    TimeMats<float>  tm32, tmT32;
+    Cart1D<double>   cart64;
+    Cart1D<float>    cart32;
+    QTab<double>     qtab64;
+    QTab<float>      qtab32;
+    DevBuf<unsigned char> shell; // tile face slots (scratch, allocated at creation)
+  };
+} // namespace stmg
