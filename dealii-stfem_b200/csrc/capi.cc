@@ -1,10 +1,14 @@
 // extern "C" entry points of libstmg_cuda.so (declared in include/stmg.h).
+#include <atomic>
 #include <cstring>
 #include <exception>
 #include <string>
 
+#include "solver.h"
 #include "st_operator.h"
 #include "stmg_internal.h"
+#include "transfer.h"
+#include "vanka.h"
 
 struct stmg_mesh_s
 {
@@ -13,6 +17,20 @@ struct stmg_mesh_s
 struct stmg_op_s
 {
   std::unique_ptr<stmg::StOperator> op;
+};
+struct stmg_vanka_s
+{
+  std::unique_ptr<stmg::Vanka> vk;
+};
+struct stmg_transfer_s
+{
+  std::unique_ptr<stmg::Transfer> tr;
+  long long                       fine_size;
+  int                             elem;
+};
+struct stmg_solver_s
+{
+  std::unique_ptr<stmg::SlabSolver> s;
 };
 
 namespace stmg
@@ -25,6 +43,21 @@ namespace stmg
   set_last_error(const std::string &m)
   {
     last_error = m;
+  }
+
+  namespace
+  {
+    std::atomic<long long> launches{0};
+  }
+  void
+  count_launch()
+  {
+    launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  long long
+  launch_count()
+  {
+    return launches.load(std::memory_order_relaxed);
   }
 
   template <typename F>
@@ -74,6 +107,15 @@ extern "C"
   stmg_version(void)
   {
     return 1;
+  }
+
+  int
+  stmg_kernel_launches(long long *count)
+  {
+    return guard([&] {
+      STMG_REQUIRE(count, STMG_ERR_ARG, "kernel_launches: null argument");
+      *count = launch_count();
+    });
   }
 
   int
@@ -170,6 +212,262 @@ extern "C"
     return guard([&] {
       STMG_REQUIRE(op && op->op, STMG_ERR_HANDLE, "op_vmult_add: null handle");
       op->op->apply(false, src, dst, true, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_vanka_create(stmg_mesh_t mesh, int nt, const double *Alpha, const double *Beta, int compute_dtype,
+                    int storage_dtype, stmg_vanka_t *vanka)
+  {
+    return guard([&] {
+      STMG_REQUIRE(mesh && mesh->m, STMG_ERR_HANDLE, "vanka_create: null mesh");
+      STMG_REQUIRE(Alpha && Beta && vanka, STMG_ERR_ARG, "vanka_create: null argument");
+      auto h = std::make_unique<stmg_vanka_s>();
+      h->vk  = std::make_unique<Vanka>(mesh->m.get(), nt, Alpha, Beta, compute_dtype, storage_dtype);
+      *vanka = h.release();
+    });
+  }
+
+  int
+  stmg_vanka_destroy(stmg_vanka_t vanka)
+  {
+    return guard([&] {
+      STMG_REQUIRE(vanka, STMG_ERR_HANDLE, "vanka_destroy: null handle");
+      delete vanka;
+    });
+  }
+
+  int
+  stmg_vanka_vmult(stmg_vanka_t vanka, void *dst, const void *src, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(vanka && vanka->vk, STMG_ERR_HANDLE, "vanka_vmult: null handle");
+      vanka->vk->apply(src, dst, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_transfer_h_create(stmg_mesh_t fine, stmg_mesh_t coarse, int nt, int dtype, stmg_transfer_t *tr)
+  {
+    return guard([&] {
+      STMG_REQUIRE(fine && fine->m && coarse && coarse->m, STMG_ERR_HANDLE, "transfer_h_create: null mesh");
+      STMG_REQUIRE(tr && (dtype == STMG_F64 || dtype == STMG_F32), STMG_ERR_ARG, "transfer_h_create: bad argument");
+      auto h       = std::make_unique<stmg_transfer_s>();
+      h->tr        = std::make_unique<HTransfer>(fine->m.get(), coarse->m.get(), nt, dtype);
+      h->fine_size = fine->m->v.N * nt;
+      h->elem      = dtype == STMG_F64 ? 8 : 4;
+      *tr          = h.release();
+    });
+  }
+
+  int
+  stmg_transfer_t_create(stmg_mesh_t mesh, int nt_fine, int nt_coarse, const double *P, const double *R, int dtype,
+                         stmg_transfer_t *tr)
+  {
+    return guard([&] {
+      STMG_REQUIRE(mesh && mesh->m, STMG_ERR_HANDLE, "transfer_t_create: null mesh");
+      STMG_REQUIRE(P && tr && (dtype == STMG_F64 || dtype == STMG_F32), STMG_ERR_ARG, "transfer_t_create: bad argument");
+      auto h       = std::make_unique<stmg_transfer_s>();
+      h->tr        = std::make_unique<TTransfer>(mesh->m.get(), nt_fine, nt_coarse, P, R, dtype);
+      h->fine_size = mesh->m->v.N * nt_fine;
+      h->elem      = dtype == STMG_F64 ? 8 : 4;
+      *tr          = h.release();
+    });
+  }
+
+  int
+  stmg_transfer_destroy(stmg_transfer_t tr)
+  {
+    return guard([&] {
+      STMG_REQUIRE(tr, STMG_ERR_HANDLE, "transfer_destroy: null handle");
+      delete tr;
+    });
+  }
+
+  int
+  stmg_transfer_prolongate(stmg_transfer_t tr, void *dst, const void *src, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(tr && tr->tr, STMG_ERR_HANDLE, "transfer_prolongate: null handle");
+      STMG_REQUIRE(dst && src, STMG_ERR_ARG, "transfer_prolongate: null vector");
+      STMG_CUDA(cudaMemsetAsync(dst, 0, tr->fine_size * tr->elem, static_cast<cudaStream_t>(stream)));
+      tr->tr->prolongate_add(src, dst, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_transfer_prolongate_add(stmg_transfer_t tr, void *dst, const void *src, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(tr && tr->tr, STMG_ERR_HANDLE, "transfer_prolongate_add: null handle");
+      STMG_REQUIRE(dst && src, STMG_ERR_ARG, "transfer_prolongate_add: null vector");
+      tr->tr->prolongate_add(src, dst, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_transfer_restrict_add(stmg_transfer_t tr, void *dst, const void *src, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(tr && tr->tr, STMG_ERR_HANDLE, "transfer_restrict_add: null handle");
+      STMG_REQUIRE(dst && src, STMG_ERR_ARG, "transfer_restrict_add: null vector");
+      tr->tr->restrict_add(src, dst, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_solver_create(const stmg_solver_config *c, stmg_solver_t *solver)
+  {
+    return guard([&] {
+      STMG_REQUIRE(c && solver, STMG_ERR_ARG, "solver_create: null argument");
+      STMG_REQUIRE(c->dim == 2 || c->dim == 3, STMG_ERR_ARG, "solver_create: dim must be 2 or 3");
+      STMG_REQUIRE(c->refine >= 0 && c->refine < 16, STMG_ERR_ARG, "solver_create: refine out of range");
+      STMG_REQUIRE(c->n_steps >= 1 && c->tau > 0, STMG_ERR_ARG, "solver_create: bad time step");
+      SolverConfig s;
+      s.dim = c->dim;
+      for (int d = 0; d < 3; ++d)
+        {
+          s.subdiv[d] = d < c->dim ? c->subdiv[d] : 1;
+          s.lo[d]     = c->lo[d];
+          s.hi[d]     = c->hi[d];
+        }
+      s.refine          = c->refine;
+      s.degree          = c->degree;
+      s.time_degree     = c->time_degree;
+      s.time_type       = c->time_type;
+      s.problem         = c->problem;
+      s.n_steps         = c->n_steps;
+      s.tau             = c->tau;
+      s.smoothing_steps = c->smoothing_steps > 0 ? c->smoothing_steps : 1;
+      s.fe_degree_min   = c->fe_degree_min;
+      s.n_steps_min     = c->n_steps_min;
+      s.mg_dtype        = c->mg_dtype;
+      s.vanka_storage   = c->vanka_storage;
+      s.tol             = c->tol;
+      s.abs_tol         = c->abs_tol;
+      s.max_iter        = c->max_iter;
+      s.restart         = c->restart > 0 ? c->restart : 30;
+      s.extrapolate     = c->extrapolate;
+      s.rhs_mode        = c->rhs_mode;
+      s.frequency       = c->frequency;
+      long long nv = 1, nc = 1, nn = 1;
+      for (int d = 0; d < c->dim; ++d)
+        {
+          const long long n = (long long)s.subdiv[d] << c->refine;
+          nv *= n + 1;
+          nc *= n;
+          nn *= n * c->degree + 1;
+        }
+      if (c->fine_vertices)
+        s.fine_vertices.assign(c->fine_vertices, c->fine_vertices + nv * c->dim);
+      if (c->fine_coeff)
+        s.fine_coeff.assign(c->fine_coeff, c->fine_coeff + nc);
+      if (c->rhs_mode == 1)
+        {
+          STMG_REQUIRE(c->f_nodal, STMG_ERR_ARG, "solver_create: rhs_mode 1 needs f_nodal");
+          s.f_nodal.assign(c->f_nodal, c->f_nodal + nn);
+        }
+      auto h = std::make_unique<stmg_solver_s>();
+      h->s   = std::make_unique<SlabSolver>(s);
+      *solver = h.release();
+    });
+  }
+
+  int
+  stmg_solver_destroy(stmg_solver_t solver)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver, STMG_ERR_HANDLE, "solver_destroy: null handle");
+      delete solver;
+    });
+  }
+
+  int
+  stmg_solver_info(stmg_solver_t solver, long long *n_nodes, int *n_blocks, int *n_levels, double *omegas)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_info: null handle");
+      if (n_nodes)
+        *n_nodes = solver->s->N;
+      if (n_blocks)
+        *n_blocks = solver->s->nb;
+      if (n_levels)
+        *n_levels = int(solver->s->gmg->levels.size());
+      if (omegas)
+        {
+          auto o = solver->s->gmg->omegas();
+          std::copy(o.begin(), o.end(), omegas);
+        }
+    });
+  }
+
+  int
+  stmg_solver_set_initial(stmg_solver_t solver, const double *u0, const double *v0)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_set_initial: null handle");
+      solver->s->set_initial(u0, v0);
+    });
+  }
+
+  int
+  stmg_solver_set_source(stmg_solver_t solver, const double *f_nodal)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_set_source: null handle");
+      STMG_REQUIRE(f_nodal, STMG_ERR_ARG, "solver_set_source: null source");
+      solver->s->set_source(f_nodal);
+    });
+  }
+
+  int
+  stmg_solver_run(stmg_solver_t solver, int n_slabs, int *iterations, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_run: null handle");
+      STMG_REQUIRE(n_slabs >= 0, STMG_ERR_ARG, "solver_run: negative slab count");
+      solver->s->run(n_slabs, iterations, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_solver_solution(stmg_solver_t solver, double *u, double *v)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_solution: null handle");
+      solver->s->download(u, v);
+    });
+  }
+
+  int
+  stmg_solver_solve(stmg_solver_t solver, double *x, const double *rhs, int *iterations, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_solve: null handle");
+      STMG_REQUIRE(x && rhs, STMG_ERR_ARG, "solver_solve: null vector");
+      const int k = solver->s->solve(x, rhs, static_cast<cudaStream_t>(stream));
+      if (iterations)
+        *iterations = k;
+    });
+  }
+
+  int
+  stmg_gmg_vmult(stmg_solver_t solver, double *dst, const double *src, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "gmg_vmult: null handle");
+      STMG_REQUIRE(dst && src, STMG_ERR_ARG, "gmg_vmult: null vector");
+      solver->s->gmg->vmult(dst, src, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_solver_system_vmult(stmg_solver_t solver, double *dst, const double *src, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_system_vmult: null handle");
+      STMG_REQUIRE(dst && src, STMG_ERR_ARG, "solver_system_vmult: null vector");
+      solver->s->system_vmult(dst, src, static_cast<cudaStream_t>(stream));
     });
   }
 }

@@ -34,7 +34,7 @@ namespace stmg
             const double *coeff)
   {
     STMG_REQUIRE(dim == 2 || dim == 3, STMG_ERR_ARG, "dim must be 2 or 3");
-    STMG_REQUIRE(p >= 1 && p <= MAX_P, STMG_ERR_UNSUPPORTED, "degree must be 1..4");
+    STMG_REQUIRE(p >= 1 && p <= MAX_P && (dim == 2 || p <= 4), STMG_ERR_UNSUPPORTED, "degree must be 1..5 (3-D: 1..4)");
     STMG_REQUIRE(coeff_mode >= 0 && coeff_mode <= 2, STMG_ERR_ARG, "coeff_mode must be 0, 1 or 2");
     STMG_REQUIRE(coeff_mode == 0 || coeff, STMG_ERR_ARG, "coefficient array missing");
     auto       m = std::make_unique<Mesh>();

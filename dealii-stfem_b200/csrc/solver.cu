@@ -1,0 +1,754 @@
+// Slab solve on the GPU (see solver.h).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "kernels_common.cuh"
+#include "solver.h"
+
+namespace stmg
+{
+  namespace
+  {
+    constexpr double PI = 3.14159265358979323846;
+
+    // ------------------------------------------------- right-hand side
+    // VectorTools::create_right_hand_side with QGauss(p+1) for the
+    // manufactured sources of tests/include/exact_solution.h:53-75 (heat)
+    // and 164-184 (wave): one thread per node gathers its cells' integrals.
+    template <int DIM, int P>
+    __global__ void
+    manufactured_rhs_kernel(const MeshView m, const __grid_constant__ QTab<double> qt, double t, double f, int wave,
+                            double *__restrict__ out)
+    {
+      constexpr int   P1   = P + 1;
+      const long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+      if (node >= m.N)
+        return;
+      const int g[3] = {int(node % m.nn[0]), int((node / m.nn[0]) % m.nn[1]), int(node / ((long long)m.nn[0] * m.nn[1]))};
+      if (is_boundary_node(m, g[0], g[1], g[2]))
+        {
+          out[node] = 0.0;
+          return;
+        }
+      const double tf = wave ? std::pow(2.0, DIM) * (PI * f) * (PI * f) * sin(2 * PI * f * t)
+                             : DIM * 4 * PI * PI * f * f * sin(2 * PI * f * t) + 2 * PI * f * cos(2 * PI * f * t);
+      int lo[3], hi[3];
+      for (int d = 0; d < 3; ++d)
+        {
+          if (d >= DIM)
+            {
+              lo[d] = hi[d] = 0;
+              continue;
+            }
+          hi[d] = min(g[d] / P, m.n[d] - 1);
+          lo[d] = (g[d] % P == 0 && g[d] > 0) ? g[d] / P - 1 : hi[d];
+        }
+      double acc = 0;
+      for (int cz = lo[2]; cz <= hi[2]; ++cz)
+        for (int cy = lo[1]; cy <= hi[1]; ++cy)
+          for (int cx = lo[0]; cx <= hi[0]; ++cx)
+            {
+              double X[1 << DIM][DIM];
+              load_corners<DIM>(m, cx, cy, cz, X);
+              const int a[3] = {g[0] - cx * P, g[1] - cy * P, DIM == 3 ? g[2] - cz * P : 0};
+              const int nq   = DIM == 3 ? P1 * P1 * P1 : P1 * P1;
+              for (int q = 0; q < nq; ++q)
+                {
+                  const int qi[3] = {q % P1, (q / P1) % P1, q / (P1 * P1)};
+                  double    xi[3] = {qt.gx[qi[0]], qt.gx[qi[1]], DIM == 3 ? qt.gx[qi[2]] : 0.0};
+                  double    J[DIM][DIM], Ji[DIM][DIM];
+                  q1_jacobian<DIM>(X, xi, J);
+                  const double det = det_inv<DIM>(J, Ji);
+                  double       w = 1, phi = 1, val = tf;
+                  for (int d = 0; d < DIM; ++d)
+                    {
+                      w *= qt.gw[qi[d]];
+                      phi *= qt.S[qi[d] * P1 + a[d]];
+                      // physical coordinate of the point (Q1 map)
+                      double x = 0;
+                      for (int v = 0; v < (1 << DIM); ++v)
+                        {
+                          double wv = 1;
+                          for (int e = 0; e < DIM; ++e)
+                            wv *= ((v >> e) & 1) ? xi[e] : 1.0 - xi[e];
+                          x += wv * X[v][d];
+                        }
+                      val *= sin(2 * PI * f * x);
+                    }
+                  acc += fabs(det) * w * phi * val;
+                }
+            }
+      out[node] = acc;
+    }
+
+    // dst (+)= sum_j C(i,j) src_j over blocks, src/dst possibly offset
+    __global__ void
+    block_combine_kernel(long long N, int n_out, int n_in, const __grid_constant__ TimeMats<double> C,
+                         const double *__restrict__ src, double *__restrict__ dst)
+    {
+      const long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+      if (node >= N)
+        return;
+      for (int i = 0; i < n_out; ++i)
+        {
+          double acc = dst[i * N + node];
+          for (int j = 0; j < n_in; ++j)
+            if (C.A[i * n_in + j] != 0.0)
+              acc += C.A[i * n_in + j] * src[j * N + node];
+          dst[i * N + node] = acc;
+        }
+    }
+
+    void
+    block_combine(long long N, const tfe::Mat &C, const double *src, double *dst, cudaStream_t s)
+    {
+      TimeMats<double> tm;
+      std::memset(&tm, 0, sizeof(tm));
+      tm.nt_out = C.m;
+      tm.nt_in  = C.n;
+      for (int i = 0; i < C.m * C.n; ++i)
+        tm.A[i] = C.a[i];
+      block_combine_kernel<<<unsigned((N + 255) / 256), 256, 0, s>>>(N, C.m, C.n, tm, src, dst);
+      count_launch();
+      STMG_CUDA(cudaGetLastError());
+    }
+
+    template <typename T>
+    T *
+    as(DevBuf<unsigned char> &b)
+    {
+      return reinterpret_cast<T *>(b.ptr);
+    }
+  } // namespace
+
+  // ------------------------------------------------------------- meshes
+  std::vector<std::unique_ptr<Mesh>>
+  build_meshes(const SolverConfig &c)
+  {
+    const int dim = c.dim, R = c.refine, p = c.degree;
+    int       nf[3] = {1, 1, 1};
+    for (int d = 0; d < dim; ++d)
+      nf[d] = c.subdiv[d] << R;
+    std::vector<std::unique_ptr<Mesh>> out;
+    for (int s = 0; s <= R; ++s)
+      {
+        const int f     = 1 << (R - s);
+        int       n[3]  = {1, 1, 1};
+        int       nv[3] = {1, 1, 1}, nvf[3] = {1, 1, 1};
+        for (int d = 0; d < dim; ++d)
+          {
+            n[d]   = nf[d] / f;
+            nv[d]  = n[d] + 1;
+            nvf[d] = nf[d] + 1;
+          }
+        std::vector<double> vert;
+        if (!c.fine_vertices.empty())
+          {
+            vert.resize(std::size_t(nv[0]) * nv[1] * nv[2] * dim);
+            for (int k = 0; k < nv[2]; ++k)
+              for (int j = 0; j < nv[1]; ++j)
+                for (int i = 0; i < nv[0]; ++i)
+                  {
+                    const std::size_t v  = i + std::size_t(nv[0]) * (j + std::size_t(nv[1]) * k);
+                    const std::size_t vf = std::size_t(i) * f + std::size_t(nvf[0]) * (std::size_t(j) * f + std::size_t(nvf[1]) * std::size_t(k) * f);
+                    for (int d = 0; d < dim; ++d)
+                      vert[v * dim + d] = c.fine_vertices[vf * dim + d];
+                  }
+          }
+        int                 mode = 0;
+        std::vector<double> coeff;
+        if (!c.fine_coeff.empty())
+          {
+            if (f == 1)
+              {
+                mode  = 1;
+                coeff = c.fine_coeff;
+              }
+            else
+              {
+                // the fine per-cell field sampled at this level's quadrature
+                // points: a point lies in fine sub-cell min(floor(xi f), f-1)
+                mode                 = 2;
+                const FETables &t    = host_tables();
+                const int       p1   = p + 1;
+                const long long ncel = (long long)n[0] * n[1] * n[2];
+                const int       nq   = dim == 3 ? p1 * p1 * p1 : p1 * p1;
+                coeff.resize(ncel * nq);
+                for (long long cc = 0; cc < ncel; ++cc)
+                  {
+                    const int ci[3] = {int(cc % n[0]), int((cc / n[0]) % n[1]), int(cc / ((long long)n[0] * n[1]))};
+                    for (int q = 0; q < nq; ++q)
+                      {
+                        const int qi[3] = {q % p1, (q / p1) % p1, q / (p1 * p1)};
+                        int       fi[3] = {0, 0, 0};
+                        for (int d = 0; d < dim; ++d)
+                          fi[d] = ci[d] * f + std::min(int(std::floor(t.gx[p][qi[d]] * f)), f - 1);
+                        coeff[cc * nq + q] = c.fine_coeff[fi[0] + std::size_t(nf[0]) * (fi[1] + std::size_t(nf[1]) * fi[2])];
+                      }
+                  }
+              }
+          }
+        out.push_back(make_mesh(dim, n, p, c.lo, c.hi, vert.empty() ? nullptr : vert.data(), mode,
+                                coeff.empty() ? nullptr : coeff.data()));
+      }
+    return out;
+  }
+
+  // ---------------------------------------------------------------- GMG
+  GMG::GMG(const SolverConfig &c, std::vector<std::unique_ptr<Mesh>> &meshes, Blas &b)
+    : dtype(c.mg_dtype)
+    , cfg(c)
+    , blas(b)
+  {
+    const auto type   = tfe::Type(c.time_type);
+    const int  lowest = type == tfe::DG ? 0 : 1;
+    int        k_min  = c.fe_degree_min < 0 ? c.time_degree - 1 : c.fe_degree_min;
+    k_min             = std::clamp(k_min, lowest, c.time_degree);
+    int n_min         = c.n_steps_min < 0 ? c.n_steps / 2 : c.n_steps_min;
+    n_min             = std::clamp(n_min, 1, c.n_steps);
+    const int n_sp    = int(meshes.size());
+    seq               = tfe::mg_sequence(n_sp, c.time_degree, k_min, c.n_steps, n_min);
+    const auto sp     = tfe::space_levels(seq, n_sp);
+    const auto w      = tfe::level_weights(type, c.problem == 2, c.time_degree, c.tau, c.n_steps, seq);
+    const int  L      = int(seq.size()) + 1;
+    levels.resize(L);
+    int r = c.time_degree, ns = c.n_steps;
+    for (int l = L - 1; l >= 0; --l)
+      {
+        if (l < L - 1)
+          {
+            if (seq[l] == tfe::K)
+              --r;
+            else if (seq[l] == tfe::TAU)
+              ns /= 2;
+          }
+        Level &lv  = levels[l];
+        lv.mesh    = meshes[sp[l]].get();
+        lv.r       = r;
+        lv.n_steps = ns;
+        lv.nt      = (type == tfe::DG ? r + 1 : r) * ns;
+        lv.A       = w[l][0];
+        lv.B       = w[l][1];
+      }
+    const std::size_t elem = dtype == STMG_F64 ? 8 : 4;
+    for (int l = 0; l < L; ++l)
+      {
+        Level &lv = levels[l];
+        lv.op     = std::make_unique<StOperator>(lv.mesh, lv.nt, lv.nt, lv.A.a.data(), lv.B.a.data(), dtype);
+        lv.vanka  = std::make_unique<Vanka>(lv.mesh, lv.nt, lv.A.a.data(), lv.B.a.data(), dtype,
+                                           dtype == STMG_F64 ? STMG_F64 : c.vanka_storage);
+        if (l > 0)
+          {
+            const Level &co = levels[l - 1];
+            if (seq[l - 1] == tfe::NONE)
+              lv.to_coarser = std::make_unique<HTransfer>(lv.mesh, co.mesh, lv.nt, dtype);
+            else
+              {
+                const tfe::Mat P = seq[l - 1] == tfe::K ? tfe::projection(type, lv.r - 1, lv.r, lv.n_steps)
+                                                        : tfe::prolongation(type, lv.r, lv.n_steps);
+                STMG_REQUIRE(P.m == lv.nt && P.n == co.nt, STMG_ERR_SHAPE, "gmg: time transfer shape");
+                lv.to_coarser = std::make_unique<TTransfer>(lv.mesh, lv.nt, co.nt, P.a.data(), nullptr, dtype);
+              }
+          }
+        const std::size_t bytes = std::size_t(lv.size()) * elem;
+        lv.sol.alloc(bytes);
+        lv.def.alloc(bytes);
+        lv.t.alloc(bytes);
+        lv.r_.alloc(bytes);
+        lv.z.alloc(bytes);
+      }
+    cudaStream_t s = nullptr;
+    for (int l = 1; l < L; ++l)
+      levels[l].omega = dtype == STMG_F64 ? estimate_relaxation<double>(l, s) : estimate_relaxation<float>(l, s);
+    STMG_CUDA(cudaDeviceSynchronize());
+  }
+
+  std::vector<double>
+  GMG::omegas() const
+  {
+    std::vector<double> o;
+    for (auto &l : levels)
+      o.push_back(l.omega);
+    return o;
+  }
+
+  unsigned
+  GMG::steps(int l) const
+  {
+    // MGSmootherPrecondition with variable = true doubles the sweeps per
+    // coarser level (gmg.h:558,726)
+    return 1u << (levels.size() - 1 - l);
+  }
+
+  // PreconditionRelaxation::step: x += omega P (b - A x)
+  template <typename T>
+  void
+  GMG::relax_step(int l, T *x, const T *b, cudaStream_t s)
+  {
+    Level          &lv = levels[l];
+    const long long n  = lv.size();
+    lv.op->apply(false, x, as<T>(lv.r_), false, s);
+    sub_from<T>(n, b, as<T>(lv.r_), s);
+    lv.vanka->apply(as<T>(lv.r_), as<T>(lv.z), s);
+    axpby<T>(n, T(lv.omega), as<T>(lv.z), T(1), x, s);
+  }
+
+  // zero_start: MGSmootherPrecondition::apply (first sweep is
+  // PreconditionRelaxation::vmult, x = omega P b); otherwise ::smooth.
+  template <typename T>
+  void
+  GMG::smooth(int l, T *x, const T *b, bool zero_start, cudaStream_t s)
+  {
+    Level          &lv = levels[l];
+    const long long n  = lv.size();
+    unsigned        k  = steps(l) * unsigned(cfg.smoothing_steps);
+    if (zero_start)
+      {
+        lv.vanka->apply(b, as<T>(lv.z), s);
+        axpby<T>(n, T(lv.omega), as<T>(lv.z), T(0), x, s);
+        --k;
+      }
+    for (unsigned i = 0; i < k; ++i)
+      relax_step<T>(l, x, b, s);
+  }
+
+  // Multigrid::level_v_step (deal.II multigrid.templates.h)
+  template <typename T>
+  void
+  GMG::vstep(int l, cudaStream_t s)
+  {
+    Level          &lv = levels[l];
+    const long long n  = lv.size();
+    if (l == 0)
+      {
+        // MGCoarseGridApplySmoother: smooth from zero
+        fill<T>(n, T(0), as<T>(lv.sol), s);
+        smooth<T>(0, as<T>(lv.sol), as<T>(lv.def), false, s);
+        return;
+      }
+    smooth<T>(l, as<T>(lv.sol), as<T>(lv.def), true, s);
+    lv.op->apply(false, as<T>(lv.sol), as<T>(lv.t), false, s);
+    sub_from<T>(n, as<T>(lv.def), as<T>(lv.t), s);
+    Level &co = levels[l - 1];
+    fill<T>(co.size(), T(0), as<T>(co.def), s);
+    lv.to_coarser->restrict_add(as<T>(lv.t), as<T>(co.def), s);
+    vstep<T>(l - 1, s);
+    lv.to_coarser->prolongate_add(as<T>(co.sol), as<T>(lv.sol), s);
+    smooth<T>(l, as<T>(lv.sol), as<T>(lv.def), false, s);
+  }
+
+  void
+  GMG::vmult(double *dst, const double *src, cudaStream_t s)
+  {
+    Level          &top = levels.back();
+    const long long n   = top.size();
+    if (dtype == STMG_F64)
+      {
+        convert<double, double>(n, src, as<double>(top.def), s);
+        vstep<double>(int(levels.size()) - 1, s);
+        convert<double, double>(n, as<double>(top.sol), dst, s);
+      }
+    else
+      {
+        convert<float, double>(n, src, as<float>(top.def), s);
+        vstep<float>(int(levels.size()) - 1, s);
+        convert<double, float>(n, as<float>(top.sol), dst, s);
+      }
+  }
+
+  // GMG::estimate_relaxation (gmg.h:792-844): power iteration with
+  // PreconditionChebyshev's start vector (all ones, entry 0 zero), 20 steps,
+  // max = 1.2 lambda, omega = 2 / (lambda + 1.2 lambda).
+  template <typename T>
+  double
+  GMG::estimate_relaxation(int l, cudaStream_t s)
+  {
+    Level          &lv = levels[l];
+    const long long n  = lv.size();
+    T              *x = as<T>(lv.sol), *y = as<T>(lv.t), *z = as<T>(lv.z);
+    fill<T>(n, T(1), x, s);
+    STMG_CUDA(cudaMemsetAsync(x, 0, sizeof(T), s));
+    double nrm = std::sqrt(blas.dot<T>(n, x, x, s));
+    axpby<T>(n, T(0), x, T(1.0 / nrm), x, s);
+    double ev = 0;
+    for (int it = 0; it < 20; ++it)
+      {
+        lv.op->apply(false, x, y, false, s);
+        lv.vanka->apply(y, z, s);
+        ev  = blas.dot<T>(n, x, z, s);
+        nrm = std::sqrt(blas.dot<T>(n, z, z, s));
+        STMG_REQUIRE(std::isfinite(nrm) && nrm > 0, STMG_ERR_NONFINITE, "gmg: power iteration broke down");
+        axpby<T>(n, T(1.0 / nrm), z, T(0), x, s);
+      }
+    ev = std::abs(ev);
+    return 2.0 / (ev + 1.2 * ev);
+  }
+
+  // -------------------------------------------------------------- FGMRES
+  FGMRES::FGMRES(long long n_, int basis_, Blas &b)
+    : n(n_)
+    , basis(basis_)
+    , blas(b)
+  {
+    STMG_REQUIRE(basis >= 2 && basis <= MAX_DOTS, STMG_ERR_ARG, "fgmres: restart length 2..32");
+    V.resize(basis);
+    Z.resize(basis);
+    for (int i = 0; i < basis; ++i)
+      {
+        V[i].alloc(n);
+        Z[i].alloc(n);
+      }
+    aux.alloc(n);
+  }
+
+  template <typename Aop, typename Pop>
+  int
+  FGMRES::solve(Aop &&A, Pop &&P, double *x, const double *b, double abs_tol, double reduce, int max_iter,
+                cudaStream_t s)
+  {
+    // Iteration k checks the residual of the k-dimensional flexible Krylov
+    // solution; a restart cycle uses at most basis-1 directions (deal.II
+    // SolverFGMRES); ReductionControl: converged if res <= abs_tol or
+    // res <= reduce * initial residual.
+    int    it          = 0;
+    double reduced_tol = -1;
+    bool   first       = true;
+    std::vector<const double *> vp(basis), zp(basis);
+    for (int i = 0; i < basis; ++i)
+      {
+        vp[i] = V[i].ptr;
+        zp[i] = Z[i].ptr;
+      }
+    while (true)
+      {
+        A(aux.ptr, x);
+        sub_from<double>(n, b, aux.ptr, s);
+        const double beta = std::sqrt(blas.dot<double>(n, aux.ptr, aux.ptr, s));
+        STMG_REQUIRE(std::isfinite(beta), STMG_ERR_NONFINITE, "fgmres: non-finite residual");
+        if (first)
+          {
+            reduced_tol      = beta * reduce;
+            initial_residual = beta;
+            first            = false;
+          }
+        last_residual = beta;
+        if (beta <= reduced_tol || beta <= abs_tol)
+          return it;
+        STMG_REQUIRE(it < max_iter, STMG_ERR_NOCONV, "fgmres: iteration limit reached");
+        std::vector<std::vector<double>> H(basis + 1, std::vector<double>(basis, 0.0));
+        std::vector<double>              cs(basis), sn(basis), g(basis + 1, 0.0);
+        g[0] = beta;
+        axpby<double>(n, 1.0 / beta, aux.ptr, 0.0, V[0].ptr, s);
+        int  used = 0;
+        bool done = false;
+        for (int j = 0; j + 1 < basis; ++j)
+          {
+            P(Z[j].ptr, V[j].ptr);
+            A(aux.ptr, Z[j].ptr);
+            // classical Gram-Schmidt, twice
+            std::vector<double> h(j + 1), h2(j + 1), neg(j + 1);
+            for (int pass = 0; pass < 2; ++pass)
+              {
+                blas.multidot<double>(n, j + 1, vp.data(), aux.ptr, (pass ? h2 : h).data(), s);
+                for (int i = 0; i <= j; ++i)
+                  neg[i] = -(pass ? h2 : h)[i];
+                blas.combine<double>(n, 1.0, j + 1, neg.data(), vp.data(), aux.ptr, s);
+              }
+            for (int i = 0; i <= j; ++i)
+              H[i][j] = h[i] + h2[i];
+            const double hn = std::sqrt(blas.dot<double>(n, aux.ptr, aux.ptr, s));
+            H[j + 1][j]     = hn;
+            if (hn != 0.0)
+              axpby<double>(n, 1.0 / hn, aux.ptr, 0.0, V[j + 1].ptr, s);
+            for (int i = 0; i < j; ++i)
+              {
+                const double t = cs[i] * H[i][j] + sn[i] * H[i + 1][j];
+                H[i + 1][j]    = -sn[i] * H[i][j] + cs[i] * H[i + 1][j];
+                H[i][j]        = t;
+              }
+            const double rr = std::hypot(H[j][j], H[j + 1][j]);
+            cs[j]           = H[j][j] / rr;
+            sn[j]           = H[j + 1][j] / rr;
+            H[j][j]         = rr;
+            H[j + 1][j]     = 0;
+            g[j + 1]        = -sn[j] * g[j];
+            g[j]            = cs[j] * g[j];
+            used            = j + 1;
+            ++it;
+            const double res = std::abs(g[j + 1]);
+            STMG_REQUIRE(std::isfinite(res), STMG_ERR_NONFINITE, "fgmres: non-finite residual");
+            last_residual = res;
+            if (res <= reduced_tol || res <= abs_tol)
+              {
+                done = true;
+                break;
+              }
+            STMG_REQUIRE(it < max_iter, STMG_ERR_NOCONV, "fgmres: iteration limit reached");
+          }
+        std::vector<double> y(used);
+        for (int i = used - 1; i >= 0; --i)
+          {
+            double acc = g[i];
+            for (int k = i + 1; k < used; ++k)
+              acc -= H[i][k] * y[k];
+            y[i] = acc / H[i][i];
+          }
+        blas.combine<double>(n, 1.0, used, y.data(), zp.data(), x, s);
+        if (done)
+          return it;
+      }
+  }
+
+  // --------------------------------------------------------- slab solver
+  SlabSolver::SlabSolver(const SolverConfig &c)
+    : cfg(c)
+  {
+    STMG_REQUIRE(c.problem == 1 || c.problem == 2, STMG_ERR_ARG, "solver: problem must be heat (1) or wave (2)");
+    STMG_REQUIRE(c.time_type == 1 || c.time_type == 2, STMG_ERR_ARG, "solver: time type must be CGP (1) or DG (2)");
+    meshes = build_meshes(c);
+    gmg    = std::make_unique<GMG>(c, meshes, blas);
+    Mesh *fine = meshes.back().get();
+    N          = fine->v.N;
+    const auto type = tfe::Type(c.time_type);
+    auto       w1a  = tfe::slab_weights(type, c.time_degree, c.tau, 1);
+    for (int i = 0; i < 4; ++i)
+      w1[i] = w1a[i];
+    ni = w1[0].m;
+    nb = ni * c.n_steps;
+    tfe::Mat lhsK, lhsM, rK, rM, rV(nb, 1);
+    if (c.problem == 2)
+      {
+        auto ww = tfe::wave_weights(type, w1[0], w1[1], w1[2], w1[3], c.n_steps);
+        lhsK = ww[0], lhsM = ww[1], rK = ww[2], rM = ww[3], rV = ww[4];
+        const tfe::Mat Ai = tfe::inverse(w1[0]);
+        AixB              = tfe::mul(Ai, w1[1]);
+        AixG              = tfe::mul(Ai, w1[2]);
+        AixZ              = tfe::mul(Ai, w1[3]);
+        for (auto &e : (type == tfe::DG ? AixG : AixZ).a)
+          e = -e;
+      }
+    else
+      {
+        auto wn = tfe::slab_weights(type, c.time_degree, c.tau, c.n_steps);
+        lhsK    = wn[0];
+        lhsM    = wn[1];
+        rK      = type == tfe::CGP ? wn[2] : tfe::Mat(nb, 1);
+        rM      = type == tfe::CGP ? wn[3] : wn[2];
+      }
+    A64   = std::make_unique<StOperator>(fine, nb, nb, lhsK.a.data(), lhsM.a.data(), STMG_F64);
+    rhs64 = std::make_unique<StOperator>(fine, nb, 1, rK.a.data(), rM.a.data(), STMG_F64);
+    if (c.problem == 2)
+      {
+        tfe::Mat zero(nb, 1);
+        rhsv64 = std::make_unique<StOperator>(fine, nb, 1, zero.a.data(), rV.a.data(), STMG_F64);
+      }
+    const double one = 1.0, zero1 = 0.0;
+    mass64 = std::make_unique<StOperator>(fine, 1, 1, &zero1, &one, STMG_F64);
+    gmres  = std::make_unique<FGMRES>(N * nb, c.restart, blas);
+    x.alloc(N * nb);
+    v.alloc(N * nb);
+    rhs.alloc(N * nb);
+    prev_x.alloc(N);
+    prev_v.alloc(N);
+    F.alloc(N);
+    STMG_CUDA(cudaMemset(x.ptr, 0, N * nb * 8));
+    STMG_CUDA(cudaMemset(v.ptr, 0, N * nb * 8));
+    // node coordinates (Q1 map of the owning cell at the Lobatto points)
+    const MeshView &m  = fine->v;
+    const FETables &tb = host_tables();
+    node_x.resize(N * m.dim);
+    const int p = m.p;
+    for (long long i = 0; i < N; ++i)
+      {
+        const long long gi[3] = {i % m.nn[0], (i / m.nn[0]) % m.nn[1], i / ((long long)m.nn[0] * m.nn[1])};
+        int             ce[3] = {0, 0, 0};
+        double          xi[3] = {0, 0, 0};
+        for (int d = 0; d < m.dim; ++d)
+          {
+            ce[d] = std::min(int(gi[d] / p), m.n[d] - 1);
+            xi[d] = tb.xs[p][gi[d] - ce[d] * p];
+          }
+        for (int d = 0; d < m.dim; ++d)
+          {
+            double acc = 0;
+            for (int vtx = 0; vtx < (1 << m.dim); ++vtx)
+              {
+                double wv = 1;
+                for (int e = 0; e < m.dim; ++e)
+                  wv *= ((vtx >> e) & 1) ? xi[e] : 1.0 - xi[e];
+                const long long vi = (ce[0] + (vtx & 1)) +
+                                     (long long)(m.n[0] + 1) * ((ce[1] + ((vtx >> 1) & 1)) +
+                                                                (m.dim == 3 ? (long long)(m.n[1] + 1) * (ce[2] + ((vtx >> 2) & 1)) : 0));
+                acc += wv * fine->vert_h[vi * m.dim + d];
+              }
+            node_x[i * m.dim + d] = acc;
+          }
+      }
+    Mf.alloc(N);
+    fsrc.alloc(N);
+    if (c.rhs_mode == 1)
+      {
+        STMG_REQUIRE((long long)c.f_nodal.size() == N, STMG_ERR_SHAPE, "solver: nodal source has wrong size");
+        set_source(c.f_nodal.data());
+      }
+    set_initial(nullptr, nullptr);
+  }
+
+  void
+  SlabSolver::set_source(const double *f_nodal)
+  {
+    STMG_REQUIRE(cfg.rhs_mode == 1, STMG_ERR_ARG, "solver: set_source needs rhs_mode 1");
+    STMG_CUDA(cudaMemcpy(fsrc.ptr, f_nodal, N * sizeof(double), cudaMemcpyHostToDevice));
+    mass64->apply(false, fsrc.ptr, Mf.ptr, false, nullptr);
+    STMG_CUDA(cudaStreamSynchronize(nullptr));
+  }
+
+  void
+  SlabSolver::set_initial(const double *u0, const double *v0)
+  {
+    const MeshView     &m = meshes.back()->v;
+    std::vector<double> hu(N, 0.0), hv(N, 0.0);
+    const double        f = cfg.frequency;
+    for (long long i = 0; i < N; ++i)
+      {
+        const long long gi[3] = {i % m.nn[0], (i / m.nn[0]) % m.nn[1], i / ((long long)m.nn[0] * m.nn[1])};
+        bool            bd    = false;
+        for (int d = 0; d < m.dim; ++d)
+          bd = bd || gi[d] == 0 || gi[d] == m.nn[d] - 1;
+        if (bd)
+          continue;
+        double su = 0, sv = 2 * PI * f; // u(0) = sin(0) ... = 0, v(0) = 2 pi f prod sin
+        for (int d = 0; d < m.dim; ++d)
+          sv *= std::sin(2 * PI * f * node_x[i * m.dim + d]);
+        hu[i] = u0 ? u0[i] : su;
+        hv[i] = v0 ? v0[i] : sv;
+      }
+    STMG_CUDA(cudaMemset(x.ptr, 0, N * nb * 8));
+    STMG_CUDA(cudaMemset(v.ptr, 0, N * nb * 8));
+    STMG_CUDA(cudaMemcpy(x.ptr + (nb - 1) * N, hu.data(), N * 8, cudaMemcpyHostToDevice));
+    if (cfg.problem == 2)
+      STMG_CUDA(cudaMemcpy(v.ptr + (nb - 1) * N, hv.data(), N * 8, cudaMemcpyHostToDevice));
+    time = 0;
+  }
+
+  void
+  SlabSolver::force(double t, double *out, cudaStream_t s)
+  {
+    const MeshView &m = meshes.back()->v;
+    if (cfg.rhs_mode == 1)
+      {
+        STMG_CUDA(cudaMemcpyAsync(out, Mf.ptr, N * 8, cudaMemcpyDeviceToDevice, s));
+        return;
+      }
+    if (cfg.rhs_mode == 2)
+      {
+        STMG_CUDA(cudaMemsetAsync(out, 0, N * 8, s));
+        return;
+      }
+    const unsigned nbk  = unsigned((N + 127) / 128);
+    const int      wave = cfg.problem == 2;
+#define STMG_RHS(D, PP)                                                                                  \
+  if (m.dim == D && m.p == PP)                                                                           \
+    {                                                                                                    \
+      manufactured_rhs_kernel<D, PP><<<nbk, 128, 0, s>>>(m, make_qtab<double>(PP), t, cfg.frequency, wave, out); \
+      STMG_CUDA(cudaGetLastError());                                                                     \
+      return;                                                                                            \
+    }
+    STMG_RHS(2, 1) STMG_RHS(2, 2) STMG_RHS(2, 3) STMG_RHS(2, 4) STMG_RHS(2, 5) STMG_RHS(3, 1) STMG_RHS(3, 2) STMG_RHS(3, 3)
+#undef STMG_RHS
+    throw Error(STMG_ERR_UNSUPPORTED, "solver: manufactured source for this dim/degree");
+      count_launch();
+  }
+
+  void
+  SlabSolver::system_vmult(double *dst, const double *src, cudaStream_t s)
+  {
+    A64->apply(false, src, dst, false, s);
+  }
+
+  int
+  SlabSolver::solve(double *xv, const double *b, cudaStream_t s)
+  {
+    auto Aop = [&](double *dst, const double *src) { A64->apply(false, src, dst, false, s); };
+    auto Pop = [&](double *dst, const double *src) { gmg->vmult(dst, src, s); };
+    return gmres->solve(Aop, Pop, xv, b, cfg.abs_tol, cfg.tol, cfg.max_iter, s);
+  }
+
+  void
+  SlabSolver::run(int n_slabs, int *its, cudaStream_t s)
+  {
+    const auto                type = tfe::Type(cfg.time_type);
+    const std::vector<double> tq   = tfe::basis_points(type, cfg.time_degree);
+    for (int slab = 0; slab < n_slabs; ++slab)
+      {
+        STMG_CUDA(cudaMemcpyAsync(prev_x.ptr, x.ptr + (nb - 1) * N, N * 8, cudaMemcpyDeviceToDevice, s));
+        if (cfg.problem == 2)
+          STMG_CUDA(cudaMemcpyAsync(prev_v.ptr, v.ptr + (nb - 1) * N, N * 8, cudaMemcpyDeviceToDevice, s));
+        // rhs (time_integrators.h:163-170 / 248-252)
+        rhs64->apply(false, prev_x.ptr, rhs.ptr, false, s);
+        if (cfg.problem == 2)
+          rhsv64->apply(false, prev_v.ptr, rhs.ptr, true, s);
+        // assemble_force (time_integrators.h:60-87)
+        for (int it = 0; it < cfg.n_steps; ++it)
+          for (int j = 0; j < int(tq.size()); ++j)
+            {
+              const double tt = time + cfg.tau * it + cfg.tau * tq[j];
+              if (cfg.rhs_mode == 2)
+                continue;
+              force(tt, F.ptr, s);
+              if (type == tfe::DG)
+                axpby<double>(N, w1[0](j, j), F.ptr, 1.0, rhs.ptr + (j + it * ni) * N, s);
+              else if (j == 0)
+                for (int i = 0; i < w1[2].m; ++i)
+                  axpby<double>(N, -w1[2](i, 0), F.ptr, 1.0, rhs.ptr + (i + it * ni) * N, s);
+              else
+                axpby<double>(N, w1[0](j - 1, j - 1), F.ptr, 1.0, rhs.ptr + (j - 1 + it * ni) * N, s);
+            }
+        // initial guess (time_integrators.h:96-104)
+        for (int b = 0; b < nb; ++b)
+          {
+            if (cfg.extrapolate)
+              STMG_CUDA(cudaMemcpyAsync(x.ptr + b * N, prev_x.ptr, N * 8, cudaMemcpyDeviceToDevice, s));
+            else
+              STMG_CUDA(cudaMemsetAsync(x.ptr + b * N, 0, N * 8, s));
+          }
+        const int k = solve(x.ptr, rhs.ptr, s);
+        if (its)
+          its[slab] = k;
+        if (cfg.problem == 2)
+          {
+            // velocity recovery (time_integrators.h:263-279)
+            STMG_CUDA(cudaMemsetAsync(v.ptr, 0, N * nb * 8, s));
+            const int ntd = AixB.m;
+            for (int it = 0; it < cfg.n_steps; ++it)
+              {
+                const double *pu = it == 0 ? prev_x.ptr : x.ptr + (it * ntd - 1) * N;
+                block_combine(N, AixB, x.ptr + it * ntd * N, v.ptr + it * ntd * N, s);
+                if (type == tfe::DG)
+                  block_combine(N, AixG, pu, v.ptr + it * ntd * N, s);
+                else
+                  {
+                    // the previous step's last velocity block; it does not
+                    // overlap the blocks written for this step
+                    const double *pv = it == 0 ? prev_v.ptr : v.ptr + (it * ntd - 1) * N;
+                    block_combine(N, AixG, pv, v.ptr + it * ntd * N, s);
+                    block_combine(N, AixZ, pu, v.ptr + it * ntd * N, s);
+                  }
+              }
+          }
+        time += cfg.n_steps * cfg.tau;
+      }
+    STMG_CUDA(cudaStreamSynchronize(s));
+  }
+
+  void
+  SlabSolver::download(double *u, double *vv) const
+  {
+    if (u)
+      STMG_CUDA(cudaMemcpy(u, x.ptr, N * nb * 8, cudaMemcpyDeviceToHost));
+    if (vv)
+      STMG_CUDA(cudaMemcpy(vv, v.ptr, N * nb * 8, cudaMemcpyDeviceToHost));
+  }
+
+} // namespace stmg

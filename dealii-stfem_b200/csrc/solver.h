@@ -1,0 +1,128 @@
+// Host C++ of the slab solve on the GPU: level hierarchy, V-cycle
+// preconditioner (GMG, tests/include/gmg.h:652-906), FP64 FGMRES
+// (SolverFGMRES with ReductionControl, time_integrators.h:44,113,174) and the
+// heat / wave slab loops (time_integrators.h:60-180,237-280).
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "blas.h"
+#include "st_operator.h"
+#include "stmg_internal.h"
+#include "time_fe.h"
+#include "transfer.h"
+#include "vanka.h"
+
+namespace stmg
+{
+  struct SolverConfig
+  {
+    int    dim = 2, subdiv[3] = {1, 1, 1}, refine = 2, degree = 2, time_degree = 1, time_type = 2, problem = 1,
+        n_steps = 1;
+    double tau = 0.125, lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+    int    smoothing_steps = 1, fe_degree_min = -1, n_steps_min = -1;
+    int    mg_dtype = STMG_F32, vanka_storage = STMG_F32;
+    double tol = 1e-12, abs_tol = 1e-12;
+    int    max_iter = 200, restart = 30, extrapolate = 1;
+    int    rhs_mode = 0; // 0 manufactured (frequency), 1 nodal source field, 2 none
+    double frequency = 1.0;
+    std::vector<double> fine_vertices, fine_coeff, f_nodal;
+  };
+
+  // One level of the space-time hierarchy (operator, smoother, transfer to
+  // the next coarser level) and its V-cycle vectors.
+  struct Level
+  {
+    Mesh                       *mesh = nullptr;
+    int                         nt   = 0, r = 0, n_steps = 0;
+    tfe::Mat                    A, B;
+    std::unique_ptr<StOperator> op;
+    std::unique_ptr<Vanka>      vanka;
+    std::unique_ptr<Transfer>   to_coarser; // between this level and level-1
+    double                      omega = 1.0;
+    DevBuf<unsigned char>       sol, def, t, r_, z;
+    long long                   size() const { return mesh->v.N * nt; }
+  };
+
+  class GMG
+  {
+  public:
+    GMG(const SolverConfig &cfg, std::vector<std::unique_ptr<Mesh>> &meshes, Blas &blas);
+    // FP64 in, FP64 out; FP32 or FP64 inside (GMG::vmult, gmg.h:846-859)
+    void vmult(double *dst, const double *src, cudaStream_t s);
+    std::vector<double> omegas() const;
+    std::vector<Level>  levels; // coarsest first
+    int                 dtype;
+    std::vector<tfe::MG> seq;
+
+  private:
+    template <typename T>
+    void vstep(int l, cudaStream_t s);
+    template <typename T>
+    void relax_step(int l, T *x, const T *b, cudaStream_t s);
+    template <typename T>
+    void smooth(int l, T *x, const T *b, bool zero_start, cudaStream_t s);
+    template <typename T>
+    double estimate_relaxation(int l, cudaStream_t s);
+    unsigned steps(int l) const;
+
+    SolverConfig cfg;
+    Blas        &blas;
+  };
+
+  // FGMRES(restart) with CGS2 orthogonalisation on device vectors.
+  class FGMRES
+  {
+  public:
+    FGMRES(long long n, int basis, Blas &blas);
+    template <typename Aop, typename Pop>
+    int solve(Aop &&A, Pop &&P, double *x, const double *b, double abs_tol, double reduce, int max_iter,
+              cudaStream_t s);
+    double last_residual = 0, initial_residual = 0;
+
+  private:
+    long long                            n;
+    int                                  basis;
+    Blas                                &blas;
+    std::vector<DevBuf<double>>          V, Z;
+    DevBuf<double>                       aux;
+  };
+
+  class SlabSolver
+  {
+  public:
+    explicit SlabSolver(const SolverConfig &cfg);
+    // initial values on the finest nodes (host); null = the manufactured
+    // solution at t = 0 (exact_solution.h:18-51,136-161)
+    void set_initial(const double *u0, const double *v0);
+    // nodal source field on the finest nodes (host): rhs = M f
+    void set_source(const double *f_nodal);
+    // run n slabs, iteration counts to `its` (host)
+    void run(int n_slabs, int *its, cudaStream_t s);
+    // one FGMRES solve of the slab system for device vectors x, rhs
+    int  solve(double *x, const double *rhs, cudaStream_t s);
+    void system_vmult(double *dst, const double *src, cudaStream_t s);
+    void download(double *u, double *v) const;
+
+    SolverConfig                        cfg;
+    std::vector<std::unique_ptr<Mesh>>  meshes; // coarsest first
+    Blas                                blas;
+    std::unique_ptr<GMG>                gmg;
+    std::unique_ptr<StOperator>         A64, rhs64, rhsv64, mass64;
+    std::unique_ptr<FGMRES>             gmres;
+    int                                 nb = 0, ni = 0;
+    long long                           N  = 0;
+    double                              time = 0;
+    tfe::Mat                            w1[4];
+    tfe::Mat                            AixB, AixG, AixZ;
+    DevBuf<double>                      x, v, prev_x, prev_v, rhs, F, Mf, fsrc;
+    std::vector<double>                 node_x; // node coordinates (host), N x dim
+    std::vector<int>                    last_iterations;
+
+  private:
+    void force(double t, double *out, cudaStream_t s);
+  };
+
+  std::vector<std::unique_ptr<Mesh>> build_meshes(const SolverConfig &cfg);
+} // namespace stmg

@@ -316,9 +316,11 @@ namespace stmg
       auto               kern = m.cartesian ? st_apply_kernel<DIM, P, T, true> : st_apply_kernel<DIM, P, T, false>;
       STMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
       kern<<<unsigned(tl.n_tiles), 256, smem, s>>>(m, tl, tm, op.cart<T>(), op.qtab<T>(), src, dst, shell, add ? 1 : 0);
+      count_launch();
       STMG_CUDA(cudaGetLastError());
       const unsigned nb = unsigned((m.N + 255) / 256);
       shell_fixup_kernel<DIM, T><<<nb, 256, 0, s>>>(m, tl, tm.nt_out, shell, dst, add ? 1 : 0);
+      count_launch();
       STMG_CUDA(cudaGetLastError());
     }
 
@@ -330,7 +332,7 @@ namespace stmg
 #define STMG_CASE(D, PP)                                                                                 \
   if (dim == D && p == PP)                                                                               \
     return launch_dp<D, PP, T>(op, transpose, src, dst, shell, add, s);
-      STMG_CASE(2, 1) STMG_CASE(2, 2) STMG_CASE(2, 3) STMG_CASE(2, 4)
+      STMG_CASE(2, 1) STMG_CASE(2, 2) STMG_CASE(2, 3) STMG_CASE(2, 4) STMG_CASE(2, 5)
       STMG_CASE(3, 1) STMG_CASE(3, 2) STMG_CASE(3, 3) STMG_CASE(3, 4)
 #undef STMG_CASE
       throw Error(STMG_ERR_UNSUPPORTED, "operator: unsupported dim/degree");

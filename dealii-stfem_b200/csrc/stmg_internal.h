@@ -14,7 +14,7 @@
 
 namespace stmg
 {
-  constexpr int MAX_P  = 4;  // spatial degrees 1..4
+  constexpr int MAX_P  = 5;  // spatial degrees 1..5 (3-D up to 4 for the operator, 3 for Vanka)
   constexpr int MAX_NT = 16; // time dofs per slab
 
   // Error carried from the implementation to the C ABI.
@@ -28,6 +28,10 @@ namespace stmg
   };
 
   void set_last_error(const std::string &m);
+
+  // Number of kernels this library has launched (diagnostic counter).
+  void      count_launch();
+  long long launch_count();
 
 #define STMG_CUDA(call)                                                                                  \
   do                                                                                                     \

@@ -1,0 +1,510 @@
+// Cell-patch space-time Vanka smoother (PreconditionVanka,
+// tests/include/gmg.h:402-540).
+//
+// The reference inverts, per cell c, the patch matrix
+//   B_c = Alpha (x) K_c + Beta (x) M_c,
+// K_c, M_c being the assembled global matrices restricted to the cell's dofs
+// (neighbour contributions included), and applies
+//   dst = sum_c R_c^T diag(1/valence) B_c^{-1} R_c src.
+// Here B_c^{-1} is applied in factored form. With the generalised
+// eigendecomposition K_c V = M_c V diag(mu), V^T M_c V = I,
+//   B_c^{-1} = (I (x) V) blockdiag_m (mu_m Alpha + Beta)^{-1} (I (x) V^T),
+// which is the same operator, so a cell stores V (nd x nd) and mu (nd)
+// instead of the (n_t nd)^2 inverse. Setup (FP64): patch assembly,
+// Cholesky of M_c, cyclic Jacobi of L^{-1} K_c L^{-T}. Apply: one pass over
+// the cells with the operator's tile / brick / shell scheme.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include <cuda_bf16.h>
+
+#include "kernels_common.cuh"
+#include "vanka.h"
+
+namespace stmg
+{
+  namespace
+  {
+    template <typename TS>
+    __device__ __forceinline__ TS
+    to_storage(double v)
+    {
+      if constexpr (std::is_same_v<TS, __nv_bfloat16>)
+        return __float2bfloat16_rn(float(v));
+      else
+        return TS(v);
+    }
+
+    // cells containing global node coordinate g along one direction
+    __device__ __forceinline__ void
+    cell_range(int g, int P, int n, int &lo, int &hi)
+    {
+      hi = min(g / P, n - 1);
+      lo = (g % P == 0 && g > 0) ? g / P - 1 : g / P;
+      lo = min(lo, n - 1);
+    }
+
+    // --------------------------------------------------------------- setup
+    // One CTA per cell: assemble K_c, M_c, factor, write V (as [m][a]) and mu.
+    template <int DIM, int P, bool CART, typename TS>
+    __global__ void
+    vanka_setup_kernel(const MeshView m, const double *__restrict__ Kref, const double *__restrict__ Mref,
+                       const double *__restrict__ elemK, const double *__restrict__ elemM, TS *__restrict__ Vout,
+                       double *__restrict__ mu_out, int *__restrict__ status)
+    {
+      constexpr int P1 = P + 1;
+      constexpr int ND = Tens<P1, DIM>::ND;
+      extern __shared__ double setup_smem[];
+      double(*K)[ND + 1] = reinterpret_cast<double(*)[ND + 1]>(setup_smem);
+      double(*M)[ND + 1] = reinterpret_cast<double(*)[ND + 1]>(setup_smem + ND * (ND + 1));
+      double(*Q)[ND + 1] = reinterpret_cast<double(*)[ND + 1]>(setup_smem + 2 * ND * (ND + 1));
+      double *rot        = setup_smem + 3 * ND * (ND + 1);
+      const long long cell = blockIdx.x;
+      const int cc[3] = {int(cell % m.n[0]), int((cell / m.n[0]) % m.n[1]), int(cell / ((long long)m.n[0] * m.n[1]))};
+      const int tid = threadIdx.x, nth = blockDim.x;
+
+      // 1. patch matrices: global K, M restricted to the cell's dofs
+      for (int e = tid; e < ND * ND; e += nth)
+        {
+          const int a = e / ND, b = e % ND;
+          const int la[3] = {a % P1, (a / P1) % P1, DIM == 3 ? a / (P1 * P1) : 0};
+          const int lb[3] = {b % P1, (b / P1) % P1, DIM == 3 ? b / (P1 * P1) : 0};
+          int       ga[3], gb[3];
+          for (int d = 0; d < 3; ++d)
+            {
+              ga[d] = cc[d] * P + la[d];
+              gb[d] = cc[d] * P + lb[d];
+            }
+          const bool bda = is_boundary_node(m, ga[0], ga[1], ga[2]);
+          const bool bdb = is_boundary_node(m, gb[0], gb[1], gb[2]);
+          double     kv = 0, mv = 0;
+          if (bda || bdb)
+            {
+              // constrained rows/columns decouple; their diagonal value
+              // never meets a nonzero input
+              if (a == b)
+                kv = mv = 1.0;
+            }
+          else
+            {
+              int lo[3], hi[3];
+              for (int d = 0; d < 3; ++d)
+                {
+                  if (d >= DIM)
+                    {
+                      lo[d] = hi[d] = 0;
+                      continue;
+                    }
+                  int l1, h1, l2, h2;
+                  cell_range(ga[d], P, m.n[d], l1, h1);
+                  cell_range(gb[d], P, m.n[d], l2, h2);
+                  lo[d] = max(l1, l2);
+                  hi[d] = min(h1, h2);
+                }
+              for (int ez = lo[2]; ez <= hi[2]; ++ez)
+                for (int ey = lo[1]; ey <= hi[1]; ++ey)
+                  for (int ex = lo[0]; ex <= hi[0]; ++ex)
+                    {
+                      const long long ec = ex + (long long)m.n[0] * (ey + (long long)m.n[1] * ez);
+                      const int       ia = (ga[0] - ex * P) + P1 * ((ga[1] - ey * P) + P1 * (DIM == 3 ? ga[2] - ez * P : 0));
+                      const int       ib = (gb[0] - ex * P) + P1 * ((gb[1] - ey * P) + P1 * (DIM == 3 ? gb[2] - ez * P : 0));
+                      if constexpr (CART)
+                        {
+                          const double kap = m.coeff_mode == 1 ? m.coeff64[ec] : 1.0;
+                          kv += kap * Kref[ia * ND + ib];
+                          mv += Mref[ia * ND + ib];
+                        }
+                      else
+                        {
+                          kv += elemK[ec * ND * ND + ia * ND + ib];
+                          mv += elemM[ec * ND * ND + ia * ND + ib];
+                        }
+                    }
+            }
+          K[a][b] = kv;
+          M[a][b] = mv;
+          Q[a][b] = a == b ? 1.0 : 0.0;
+        }
+      __syncthreads();
+
+      // 2. Cholesky M = L L^T (lower triangle of M)
+      for (int j = 0; j < ND; ++j)
+        {
+          if (tid == 0)
+            {
+              double s = M[j][j];
+              for (int k = 0; k < j; ++k)
+                s -= M[j][k] * M[j][k];
+              if (!(s > 0))
+                atomicExch(status, 1);
+              M[j][j] = sqrt(fmax(s, 1e-300));
+            }
+          __syncthreads();
+          for (int i = j + 1 + tid; i < ND; i += nth)
+            {
+              double s = M[i][j];
+              for (int k = 0; k < j; ++k)
+                s -= M[i][k] * M[j][k];
+              M[i][j] = s / M[j][j];
+            }
+          __syncthreads();
+        }
+      // 3. K <- L^{-1} K L^{-T}: forward substitution on columns, then rows
+      for (int col = tid; col < ND; col += nth)
+        for (int i = 0; i < ND; ++i)
+          {
+            double s = K[i][col];
+            for (int k = 0; k < i; ++k)
+              s -= M[i][k] * K[k][col];
+            K[i][col] = s / M[i][i];
+          }
+      __syncthreads();
+      for (int row = tid; row < ND; row += nth)
+        for (int i = 0; i < ND; ++i)
+          {
+            double s = K[row][i];
+            for (int k = 0; k < i; ++k)
+              s -= M[i][k] * K[row][k];
+            K[row][i] = s / M[i][i];
+          }
+      __syncthreads();
+      // symmetrise (rounding)
+      for (int e = tid; e < ND * ND; e += nth)
+        {
+          const int a = e / ND, b = e % ND;
+          if (a < b)
+            {
+              const double v = 0.5 * (K[a][b] + K[b][a]);
+              K[a][b]        = v;
+              K[b][a]        = v;
+            }
+        }
+      __syncthreads();
+
+      // 4. parallel cyclic Jacobi, K = Q diag(mu) Q^T: each round applies
+      //    the m/2 disjoint rotations of a round-robin tournament (index 0
+      //    fixed, the others rotating; an odd ND gets a dummy index ND), as
+      //    K <- J^T (K J), Q <- Q J.
+      constexpr int MJ = (ND % 2) ? ND + 1 : ND;
+      constexpr int NP = MJ / 2;
+      int    *rp = reinterpret_cast<int *>(rot + 4);
+      double *rc = rot + 4 + NP, *rs = rc + NP;
+      for (int sweep = 0; sweep < 40; ++sweep)
+        {
+          if (tid == 0)
+            {
+              double off = 0, dg = 0;
+              for (int a = 0; a < ND; ++a)
+                {
+                  dg += K[a][a] * K[a][a];
+                  for (int b = a + 1; b < ND; ++b)
+                    off += K[a][b] * K[a][b];
+                }
+              rot[3] = (off <= 1e-30 * dg) ? 1.0 : 0.0;
+            }
+          __syncthreads();
+          if (rot[3] != 0.0)
+            break;
+          for (int round = 0; round < MJ - 1; ++round)
+            {
+              for (int k = tid; k < NP; k += nth)
+                {
+                  const int ia = k, ib = MJ - 1 - k;
+                  const int pa = ia == 0 ? 0 : ((ia - 1 + round) % (MJ - 1)) + 1;
+                  const int pb = ((ib - 1 + round) % (MJ - 1)) + 1;
+                  const int p  = min(pa, pb), q = max(pa, pb);
+                  double    c = 1, sn = 0;
+                  if (q < ND)
+                    {
+                      const double apq = K[p][q];
+                      if (apq != 0.0)
+                        {
+                          const double th = (K[q][q] - K[p][p]) / (2.0 * apq);
+                          const double t  = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                          c               = 1.0 / sqrt(t * t + 1.0);
+                          sn              = t * c;
+                        }
+                    }
+                  rp[2 * k]     = p;
+                  rp[2 * k + 1] = q;
+                  rc[k]         = c;
+                  rs[k]         = sn;
+                }
+              __syncthreads();
+              // columns: K <- K J, Q <- Q J (row i owned by one thread)
+              for (int i = tid; i < ND; i += nth)
+                for (int k = 0; k < NP; ++k)
+                  {
+                    const int q = rp[2 * k + 1];
+                    if (q >= ND || rs[k] == 0.0)
+                      continue;
+                    const int    p = rp[2 * k];
+                    const double c = rc[k], sn = rs[k];
+                    const double kp = K[i][p], kq = K[i][q];
+                    K[i][p]         = c * kp - sn * kq;
+                    K[i][q]         = sn * kp + c * kq;
+                    const double qp = Q[i][p], qq = Q[i][q];
+                    Q[i][p]         = c * qp - sn * qq;
+                    Q[i][q]         = sn * qp + c * qq;
+                  }
+              __syncthreads();
+              // rows: K <- J^T K (pair k, column j)
+              for (int e = tid; e < NP * ND; e += nth)
+                {
+                  const int k = e / ND, j = e % ND;
+                  const int q = rp[2 * k + 1];
+                  if (q >= ND || rs[k] == 0.0)
+                    continue;
+                  const int    p = rp[2 * k];
+                  const double c = rc[k], sn = rs[k];
+                  const double kp = K[p][j], kq = K[q][j];
+                  K[p][j]         = c * kp - sn * kq;
+                  K[q][j]         = sn * kp + c * kq;
+                }
+              __syncthreads();
+            }
+        }
+      // 5. V = L^{-T} Q (back substitution per column), store as [m][a]
+      for (int col = tid; col < ND; col += nth)
+        {
+          for (int i = ND - 1; i >= 0; --i)
+            {
+              double s = Q[i][col];
+              for (int k = i + 1; k < ND; ++k)
+                s -= M[k][i] * Q[k][col];
+              Q[i][col] = s / M[i][i];
+            }
+          mu_out[cell * ND + col] = K[col][col];
+        }
+      __syncthreads();
+      for (int e = tid; e < ND * ND; e += nth)
+        {
+          const int mm = e / ND, a = e % ND;
+          Vout[cell * ND * ND + e] = to_storage<TS>(Q[a][mm]);
+        }
+    }
+
+    // Element matrices of every cell for the general (non-cartesian) path.
+    template <int DIM, int P>
+    __global__ void
+    element_matrix_kernel(const MeshView m, const __grid_constant__ QTab<double> qt, double *__restrict__ Ke,
+                          double *__restrict__ Me)
+    {
+      constexpr int P1 = P + 1;
+      constexpr int ND = Tens<P1, DIM>::ND;
+      const long long cell = blockIdx.x;
+      const int cc[3] = {int(cell % m.n[0]), int((cell / m.n[0]) % m.n[1]), int(cell / ((long long)m.n[0] * m.n[1]))};
+      __shared__ double G[ND][DIM * DIM], W[ND];
+      double X[1 << DIM][DIM];
+      load_corners<DIM>(m, cc[0], cc[1], cc[2], X);
+      for (int q = threadIdx.x; q < ND; q += blockDim.x)
+        {
+          const int qx = q % P1, qy = (q / P1) % P1, qz = q / (P1 * P1);
+          double    xi[3] = {qt.gx[qx], qt.gx[qy], DIM == 3 ? qt.gx[qz] : 0.0};
+          double    J[DIM][DIM], Ji[DIM][DIM];
+          q1_jacobian<DIM>(X, xi, J);
+          const double det = det_inv<DIM>(J, Ji);
+          double       w   = qt.gw[qx] * qt.gw[qy] * (DIM == 3 ? qt.gw[qz] : 1.0);
+          const double JxW = fabs(det) * w;
+          const double k = m.coeff_mode == 1 ? m.coeff64[cell] : (m.coeff_mode == 2 ? m.coeff64[cell * ND + q] : 1.0);
+          for (int a = 0; a < DIM; ++a)
+            for (int b = 0; b < DIM; ++b)
+              {
+                double s = 0;
+                for (int i = 0; i < DIM; ++i)
+                  s += Ji[a][i] * Ji[b][i];
+                G[q][a * DIM + b] = k * JxW * s;
+              }
+          W[q] = JxW;
+        }
+      __syncthreads();
+      // reference gradients of basis function a at point q via S, D tables:
+      // phi_a(q) = prod S, d_j phi_a(q) = D in direction j
+      for (int e = threadIdx.x; e < ND * ND; e += blockDim.x)
+        {
+          const int a = e / ND, b = e % ND;
+          const int ai[3] = {a % P1, (a / P1) % P1, a / (P1 * P1)};
+          const int bi[3] = {b % P1, (b / P1) % P1, b / (P1 * P1)};
+          double    kv = 0, mv = 0;
+          for (int q = 0; q < ND; ++q)
+            {
+              const int qi[3] = {q % P1, (q / P1) % P1, q / (P1 * P1)};
+              double    pa = 1, pb = 1, ga[DIM], gb[DIM];
+              for (int j = 0; j < DIM; ++j)
+                ga[j] = gb[j] = 1;
+              for (int d = 0; d < DIM; ++d)
+                {
+                  const double sa = qt.S[qi[d] * P1 + ai[d]], sb = qt.S[qi[d] * P1 + bi[d]];
+                  // D = Dq S (collocation): d phi_a / d xi_d at q
+                  double da = 0, db = 0;
+                  for (int r = 0; r < P1; ++r)
+                    {
+                      da += qt.Dq[qi[d] * P1 + r] * qt.S[r * P1 + ai[d]];
+                      db += qt.Dq[qi[d] * P1 + r] * qt.S[r * P1 + bi[d]];
+                    }
+                  pa *= sa;
+                  pb *= sb;
+                  for (int j = 0; j < DIM; ++j)
+                    {
+                      ga[j] *= (j == d) ? da : sa;
+                      gb[j] *= (j == d) ? db : sb;
+                    }
+                }
+              mv += W[q] * pa * pb;
+              for (int i = 0; i < DIM; ++i)
+                for (int j = 0; j < DIM; ++j)
+                  kv += ga[i] * G[q][i * DIM + j] * gb[j];
+            }
+          Ke[cell * ND * ND + e] = kv;
+          Me[cell * ND * ND + e] = mv;
+        }
+    }
+
+  } // namespace
+
+  // ------------------------------------------------------------------ host
+  std::size_t
+  Vanka::smem_bytes(const Tiling &tl) const
+  {
+    const std::size_t elem = compute == STMG_F64 ? 8 : 4;
+    return elem * (std::size_t(nt) * tl.E[0] * tl.E[1] * tl.E[2] + 2ull * tl.T[0] * tl.T[1] * tl.T[2] * nt * mesh->nd);
+  }
+
+  namespace
+  {
+    template <int DIM, int P>
+    void
+    run_setup(Vanka &vk)
+    {
+      constexpr int   ND = Tens<P + 1, DIM>::ND;
+      const MeshView &m  = vk.mesh->v;
+      DevBuf<int>     status(1);
+      STMG_CUDA(cudaMemset(status.ptr, 0, sizeof(int)));
+      DevBuf<double> Kref, Mref, eK, eM, mu64(m.ncells * ND);
+      const int      threads = ND <= 32 ? 32 : 64;
+      if (m.cartesian)
+        {
+          // reference element matrices of the level's cell size (kappa = 1)
+          const FETables     &t = host_tables();
+          std::vector<double> k(ND * ND), mm(ND * ND);
+          for (int a = 0; a < ND; ++a)
+            for (int b = 0; b < ND; ++b)
+              {
+                const int ai[3] = {a % (P + 1), (a / (P + 1)) % (P + 1), a / ((P + 1) * (P + 1))};
+                const int bi[3] = {b % (P + 1), (b / (P + 1)) % (P + 1), b / ((P + 1) * (P + 1))};
+                double    mv = 1, kv = 0;
+                for (int d = 0; d < DIM; ++d)
+                  mv *= t.M1[P][ai[d]][bi[d]] * m.h[d];
+                for (int j = 0; j < DIM; ++j)
+                  {
+                    double term = 1;
+                    for (int d = 0; d < DIM; ++d)
+                      term *= d == j ? t.K1[P][ai[d]][bi[d]] / m.h[d] : t.M1[P][ai[d]][bi[d]] * m.h[d];
+                    kv += term;
+                  }
+                k[a * ND + b]  = kv;
+                mm[a * ND + b] = mv;
+              }
+          Kref.upload(k);
+          Mref.upload(mm);
+        }
+      else
+        {
+          eK.alloc(m.ncells * ND * ND);
+          eM.alloc(m.ncells * ND * ND);
+          element_matrix_kernel<DIM, P><<<unsigned(m.ncells), 64>>>(m, make_qtab<double>(P), eK.ptr, eM.ptr);
+          count_launch();
+          STMG_CUDA(cudaGetLastError());
+        }
+      const std::size_t smem = (3ull * ND * (ND + 1) + 4 + 3 * ((ND + 1) / 2 + 1)) * sizeof(double);
+      auto go = [&](auto *Vp) {
+        using TS  = std::remove_pointer_t<decltype(Vp)>;
+        auto kern = m.cartesian ? vanka_setup_kernel<DIM, P, true, TS> : vanka_setup_kernel<DIM, P, false, TS>;
+        STMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        kern<<<unsigned(m.ncells), threads, smem>>>(m, Kref.ptr, Mref.ptr, eK.ptr, eM.ptr, Vp, mu64.ptr, status.ptr);
+        count_launch();
+        STMG_CUDA(cudaGetLastError());
+      };
+      if (vk.storage == STMG_F64)
+        go(reinterpret_cast<double *>(vk.V.ptr));
+      else if (vk.storage == STMG_F32)
+        go(reinterpret_cast<float *>(vk.V.ptr));
+      else
+        go(reinterpret_cast<__nv_bfloat16 *>(vk.V.ptr));
+      STMG_CUDA(cudaDeviceSynchronize());
+      int st = 0;
+      STMG_CUDA(cudaMemcpy(&st, status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+      STMG_REQUIRE(st == 0, STMG_ERR_NONFINITE, "vanka setup: patch mass matrix not positive definite");
+      if (vk.compute == STMG_F64)
+        {
+          vk.mu.alloc(m.ncells * ND * 8);
+          STMG_CUDA(cudaMemcpy(vk.mu.ptr, mu64.ptr, m.ncells * ND * 8, cudaMemcpyDeviceToDevice));
+        }
+      else
+        {
+          std::vector<double> h(m.ncells * ND);
+          STMG_CUDA(cudaMemcpy(h.data(), mu64.ptr, h.size() * 8, cudaMemcpyDeviceToHost));
+          std::vector<float> f(h.begin(), h.end());
+          vk.mu.alloc(f.size() * 4);
+          STMG_CUDA(cudaMemcpy(vk.mu.ptr, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+        }
+    }
+
+  } // namespace
+
+  Vanka::Vanka(Mesh *mesh_, int nt_, const double *A, const double *B, int compute_, int storage_)
+    : mesh(mesh_)
+    , nt(nt_)
+    , compute(compute_)
+    , storage(storage_)
+  {
+    STMG_REQUIRE(nt >= 1 && nt <= MAX_NT, STMG_ERR_ARG, "vanka: time dofs must be 1..16");
+    STMG_REQUIRE(compute == STMG_F64 || compute == STMG_F32, STMG_ERR_ARG, "vanka: compute type F64 or F32");
+    STMG_REQUIRE(compute == STMG_F32 ? (storage == STMG_F32 || storage == STMG_BF16) : storage == STMG_F64,
+                 STMG_ERR_ARG, "vanka: storage F32/BF16 with F32 compute, F64 with F64 compute");
+    const int dim = mesh->v.dim, p = mesh->v.p;
+    STMG_REQUIRE(!(dim == 3 && p > 3), STMG_ERR_UNSUPPORTED, "vanka: 3-D degree up to 3");
+    std::memset(&tm64, 0, sizeof(tm64));
+    std::memset(&tm32, 0, sizeof(tm32));
+    tm64.nt_out = tm64.nt_in = tm32.nt_out = tm32.nt_in = nt;
+    for (int i = 0; i < nt * nt; ++i)
+      {
+        tm64.A[i] = A[i];
+        tm64.B[i] = B[i];
+        tm32.A[i] = float(A[i]);
+        tm32.B[i] = float(B[i]);
+      }
+    const std::size_t nd   = mesh->nd;
+    const std::size_t elem = storage == STMG_F64 ? 8 : (storage == STMG_F32 ? 4 : 2);
+    V.alloc(std::size_t(mesh->v.ncells) * nd * nd * elem);
+#define STMG_SETUP(D, PP)                                                                                \
+  if (dim == D && p == PP)                                                                               \
+    run_setup<D, PP>(*this);
+    STMG_SETUP(2, 1) STMG_SETUP(2, 2) STMG_SETUP(2, 3) STMG_SETUP(2, 4) STMG_SETUP(2, 5)
+    STMG_SETUP(3, 1) STMG_SETUP(3, 2) STMG_SETUP(3, 3)
+#undef STMG_SETUP
+    // tiling within a shared-memory budget
+    static const int cand3[][3] = {{8, 4, 4}, {4, 4, 4}, {4, 4, 2}, {4, 2, 2}, {2, 2, 2}, {2, 2, 1}, {2, 1, 1}, {1, 1, 1}};
+    static const int cand2[][3] = {{16, 8, 1}, {8, 8, 1}, {8, 4, 1}, {4, 4, 1}, {4, 2, 1}, {2, 2, 1}, {2, 1, 1}, {1, 1, 1}};
+    bool ok = false;
+    for (int k = 0; k < 8 && !ok; ++k)
+      {
+        tiling = make_tiling(mesh->v, dim == 3 ? cand3[k] : cand2[k]);
+        ok     = smem_bytes(tiling) <= 100 * 1024;
+      }
+    STMG_REQUIRE(ok, STMG_ERR_UNSUPPORTED, "vanka: does not fit in shared memory");
+    shell.alloc(std::size_t(tiling.n_tiles) * nt * tiling.tile_stride * (compute == STMG_F64 ? 8 : 4));
+  }
+
+  void
+  Vanka::apply(const void *src, void *dst, cudaStream_t s) const
+  {
+    STMG_REQUIRE(src && dst, STMG_ERR_ARG, "vanka: null vector");
+    const int dim = mesh->v.dim, p = mesh->v.p;
+    (void)p;
+    if (dim == 2)
+      return vanka_apply_2d(*this, src, dst, s);
+    return vanka_apply_3d(*this, src, dst, s);
+  }
+} // namespace stmg

@@ -58,6 +58,12 @@ def check(rc):
         raise StmgError(rc, lib().stmg_last_error().decode())
 
 
+def kernel_launches():
+    n = C.c_longlong()
+    check(lib().stmg_kernel_launches(C.byref(n)))
+    return n.value
+
+
 def _ptr(a):
     if a is None:
         return None
@@ -128,3 +134,148 @@ class Operator:
 
     def vmult_add(self, dst, src, stream=None):
         check(lib().stmg_op_vmult_add(self.h, _dev(dst), _dev(src), _stream(stream)))
+
+
+class Vanka:
+    """stmg_vanka_t: cell-patch space-time Vanka smoother of one level."""
+
+    def __init__(self, mesh, Alpha, Beta, compute=F32, storage=None):
+        A = np.ascontiguousarray(Alpha, dtype=np.float64)
+        B = np.ascontiguousarray(Beta, dtype=np.float64)
+        if storage is None:
+            storage = compute
+        self.mesh, self.nt = mesh, A.shape[0]
+        h = C.c_void_p()
+        check(lib().stmg_vanka_create(mesh.h, self.nt, _ptr(A), _ptr(B), compute, storage, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.stmg_vanka_destroy(self.h)
+            self.h = None
+
+    def vmult(self, dst, src, stream=None):
+        check(lib().stmg_vanka_vmult(self.h, _dev(dst), _dev(src), _stream(stream)))
+
+
+class Transfer:
+    """stmg_transfer_t: h-transfer (fine, coarse meshes) or time transfer (P)."""
+
+    def __init__(self, fine=None, coarse=None, nt=1, dtype=F64, mesh=None, P=None, R=None):
+        h = C.c_void_p()
+        if P is None:
+            check(lib().stmg_transfer_h_create(fine.h, coarse.h, nt, dtype, C.byref(h)))
+        else:
+            P = np.ascontiguousarray(P, dtype=np.float64)
+            Rm = None if R is None else np.ascontiguousarray(R, dtype=np.float64)
+            self._keep = (P, Rm)
+            check(lib().stmg_transfer_t_create(mesh.h, P.shape[0], P.shape[1], _ptr(P), _ptr(Rm), dtype, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.stmg_transfer_destroy(self.h)
+            self.h = None
+
+    def prolongate(self, dst, src, stream=None):
+        check(lib().stmg_transfer_prolongate(self.h, _dev(dst), _dev(src), _stream(stream)))
+
+    def prolongate_add(self, dst, src, stream=None):
+        check(lib().stmg_transfer_prolongate_add(self.h, _dev(dst), _dev(src), _stream(stream)))
+
+    def restrict_add(self, dst, src, stream=None):
+        check(lib().stmg_transfer_restrict_add(self.h, _dev(dst), _dev(src), _stream(stream)))
+
+
+class SolverConfig(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("subdiv", C.c_int * 3), ("refine", C.c_int), ("degree", C.c_int),
+        ("time_degree", C.c_int), ("time_type", C.c_int), ("problem", C.c_int), ("n_steps", C.c_int),
+        ("tau", C.c_double), ("lo", C.c_double * 3), ("hi", C.c_double * 3),
+        ("smoothing_steps", C.c_int), ("fe_degree_min", C.c_int), ("n_steps_min", C.c_int),
+        ("mg_dtype", C.c_int), ("vanka_storage", C.c_int),
+        ("tol", C.c_double), ("abs_tol", C.c_double),
+        ("max_iter", C.c_int), ("restart", C.c_int), ("extrapolate", C.c_int),
+        ("rhs_mode", C.c_int), ("frequency", C.c_double),
+        ("fine_vertices", _dp), ("fine_coeff", _dp), ("f_nodal", _dp),
+    ]
+
+
+class Solver:
+    """stmg_solver_t: FP64 FGMRES + space-time V-cycle slab solver."""
+
+    def __init__(self, dim=2, subdiv=(1, 1, 1), refine=2, degree=2, time_degree=1, time_type=DG, problem=HEAT,
+                 n_steps=1, tau=None, lo=(0, 0, 0), hi=(1, 1, 1), smoothing_steps=1, fe_degree_min=-1,
+                 n_steps_min=-1, mg_dtype=F32, vanka_storage=None, tol=1e-12, abs_tol=1e-12, max_iter=200,
+                 restart=30, extrapolate=True, rhs_mode=0, frequency=1.0, fine_vertices=None, fine_coeff=None,
+                 f_nodal=None):
+        c = SolverConfig()
+        c.dim, c.refine, c.degree, c.time_degree = dim, refine, degree, time_degree
+        c.subdiv[:] = list(subdiv) + [1] * (3 - len(subdiv))
+        c.time_type, c.problem, c.n_steps = time_type, problem, n_steps
+        c.tau = 2.0 ** -(refine + 1) if tau is None else tau
+        c.lo[:] = list(lo) + [0] * (3 - len(lo))
+        c.hi[:] = list(hi) + [1] * (3 - len(hi))
+        c.smoothing_steps, c.fe_degree_min, c.n_steps_min = smoothing_steps, fe_degree_min, n_steps_min
+        c.mg_dtype = mg_dtype
+        c.vanka_storage = mg_dtype if vanka_storage is None else vanka_storage
+        c.tol, c.abs_tol, c.max_iter, c.restart, c.extrapolate = tol, abs_tol, max_iter, restart, int(extrapolate)
+        c.rhs_mode, c.frequency = rhs_mode, frequency
+        keep = []
+
+        def arr(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            return _ptr(a)
+
+        c.fine_vertices, c.fine_coeff, c.f_nodal = arr(fine_vertices), arr(fine_coeff), arr(f_nodal)
+        h = C.c_void_p()
+        check(lib().stmg_solver_create(C.byref(c), C.byref(h)))
+        self.h, self.cfg, self.tau = h, c, c.tau
+        nn, nb, nl = C.c_longlong(), C.c_int(), C.c_int()
+        check(lib().stmg_solver_info(self.h, C.byref(nn), C.byref(nb), C.byref(nl), None))
+        self.n_nodes, self.n_blocks, self.n_levels = nn.value, nb.value, nl.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.stmg_solver_destroy(self.h)
+            self.h = None
+
+    def omegas(self):
+        o = np.zeros(self.n_levels)
+        check(lib().stmg_solver_info(self.h, None, None, None, _ptr(o)))
+        return o
+
+    def set_initial(self, u0=None, v0=None):
+        u = None if u0 is None else np.ascontiguousarray(u0, dtype=np.float64)
+        v = None if v0 is None else np.ascontiguousarray(v0, dtype=np.float64)
+        check(lib().stmg_solver_set_initial(self.h, _ptr(u), _ptr(v)))
+
+    def set_source(self, f_nodal):
+        f = np.ascontiguousarray(f_nodal, dtype=np.float64)
+        check(lib().stmg_solver_set_source(self.h, _ptr(f)))
+
+    def run(self, n_slabs, stream=None):
+        its = np.zeros(n_slabs, dtype=np.int32)
+        check(lib().stmg_solver_run(self.h, n_slabs, its.ctypes.data_as(_ip), _stream(stream)))
+        return its
+
+    def solution(self):
+        u = np.zeros(self.n_blocks * self.n_nodes)
+        v = np.zeros(self.n_blocks * self.n_nodes)
+        check(lib().stmg_solver_solution(self.h, _ptr(u), _ptr(v)))
+        return u, v
+
+    def solve(self, x, rhs, stream=None):
+        k = C.c_int()
+        check(lib().stmg_solver_solve(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(rhs.data_ptr()), C.byref(k),
+                                      _stream(stream)))
+        return k.value
+
+    def gmg_vmult(self, dst, src, stream=None):
+        check(lib().stmg_gmg_vmult(self.h, _dev(dst), _dev(src), _stream(stream)))
+
+    def system_vmult(self, dst, src, stream=None):
+        check(lib().stmg_solver_system_vmult(self.h, _dev(dst), _dev(src), _stream(stream)))

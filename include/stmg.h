@@ -53,6 +53,9 @@ enum
 
 STMG_API const char *stmg_last_error(void);
 STMG_API int         stmg_version(void);
+/* Number of CUDA kernels the library has launched since it was loaded.
+ * Diagnostic counter with no counterpart in the reference. */
+STMG_API int stmg_kernel_launches(long long *count);
 
 /* ---------------------------------------------------------------- mesh
  * Structured hex mesh of n_cells[0] x n_cells[1] (x n_cells[2]) cells of
@@ -83,6 +86,82 @@ STMG_API int stmg_op_vmult(stmg_op_t op, void *dst, const void *src, void *strea
 STMG_API int stmg_op_Tvmult(stmg_op_t op, void *dst, const void *src, void *stream);
 /* SystemMatrix::vmult_add (operators.h:155-180): dst += op(src). */
 STMG_API int stmg_op_vmult_add(stmg_op_t op, void *dst, const void *src, void *stream);
+
+/* ---------------------------------------------------------------- Vanka
+ * Cell-patch space-time Vanka smoother of one level: per cell the inverse of
+ * Alpha (x) K_c + Beta (x) M_c with K_c, M_c the assembled matrices restricted
+ * to the cell's dofs, applied in factored form (generalised eigenvectors of
+ * (K_c, M_c) and per-mode n_t x n_t solves), contributions weighted by
+ * 1/valence. compute STMG_F32 with storage STMG_F32 or STMG_BF16, or
+ * STMG_F64 with STMG_F64. Replaces PreconditionVanka's constructor
+ * (gmg.h:409-474). */
+STMG_API int stmg_vanka_create(stmg_mesh_t mesh, int nt, const double *Alpha, const double *Beta, int compute_dtype,
+                               int storage_dtype, stmg_vanka_t *vanka);
+STMG_API int stmg_vanka_destroy(stmg_vanka_t vanka);
+/* PreconditionVanka::vmult (gmg.h:476-514): dst = sum_c R_c^T D_c B_c^{-1} R_c src. */
+STMG_API int stmg_vanka_vmult(stmg_vanka_t vanka, void *dst, const void *src, void *stream);
+
+/* ------------------------------------------------------------ transfers
+ * h: between a mesh and its 2x refinement (same degree), nt time blocks;
+ * replaces MGTwoLevelBlockTransfer over deal.II's MGTwoLevelTransfer
+ * (gmg.h:35-75, built at gmg.h:369-380).
+ * t: (P (x) I) on one mesh, P nt_fine x nt_coarse, R nt_coarse x nt_fine or
+ * NULL for P^T; replaces MGTwoLevelTransferST (gmg.h:77-136). */
+STMG_API int stmg_transfer_h_create(stmg_mesh_t fine, stmg_mesh_t coarse, int nt, int dtype, stmg_transfer_t *tr);
+STMG_API int stmg_transfer_t_create(stmg_mesh_t mesh, int nt_fine, int nt_coarse, const double *P, const double *R,
+                                    int dtype, stmg_transfer_t *tr);
+STMG_API int stmg_transfer_destroy(stmg_transfer_t tr);
+/* STMGTransferBlockMatrixFree::prolongate (gmg.h:195-201): dst = P src. */
+STMG_API int stmg_transfer_prolongate(stmg_transfer_t tr, void *dst, const void *src, void *stream);
+/* ::prolongate_and_add (gmg.h:203-209): dst += P src. */
+STMG_API int stmg_transfer_prolongate_add(stmg_transfer_t tr, void *dst, const void *src, void *stream);
+/* ::restrict_and_add (gmg.h:211-217): dst += R src. */
+STMG_API int stmg_transfer_restrict_add(stmg_transfer_t tr, void *dst, const void *src, void *stream);
+
+/* --------------------------------------------------------------- solver
+ * Slab solver of the heat (problem 1) or condensed wave (problem 2) system:
+ * FP64 FGMRES preconditioned by the space-time V-cycle (FP32 or FP64) on
+ * the structured mesh of subdiv cells refined `refine` times (levels as
+ * tests/tp_01.cc:200-359 builds them). time_type 1 = cGP, 2 = dG. */
+typedef struct
+{
+  int           dim, subdiv[3], refine, degree, time_degree, time_type, problem, n_steps;
+  double        tau, lo[3], hi[3];
+  int           smoothing_steps, fe_degree_min, n_steps_min; /* -1: reference defaults */
+  int           mg_dtype, vanka_storage;                      /* STMG_F32/F64; STMG_F32/BF16/F64 */
+  double        tol, abs_tol;                                 /* ReductionControl reduce, tolerance */
+  int           max_iter, restart, extrapolate;
+  int           rhs_mode; /* 0 manufactured (frequency), 1 nodal source f_nodal, 2 none */
+  double        frequency;
+  const double *fine_vertices; /* NULL or finest-mesh vertices */
+  const double *fine_coeff;    /* NULL or per finest cell */
+  const double *f_nodal;       /* rhs_mode 1: finest nodal values */
+} stmg_solver_config;
+
+STMG_API int stmg_solver_create(const stmg_solver_config *cfg, stmg_solver_t *solver);
+STMG_API int stmg_solver_destroy(stmg_solver_t solver);
+/* sizes; omegas (n_levels values, may be NULL) are the relaxation factors of
+ * GMG::estimate_relaxation (gmg.h:792-844) */
+STMG_API int stmg_solver_info(stmg_solver_t solver, long long *n_nodes, int *n_blocks, int *n_levels, double *omegas);
+/* initial u, v on the finest nodes (host arrays of n_nodes, NULL = the
+ * manufactured solution at t = 0); resets time to 0 */
+STMG_API int stmg_solver_set_initial(stmg_solver_t solver, const double *u0, const double *v0);
+/* replace the nodal source field (host array of n_nodes; rhs_mode 1): the
+ * integrate_rhs_function of tests/tp_01.cc:390-398 for an FE source */
+STMG_API int stmg_solver_set_source(stmg_solver_t solver, const double *f_nodal);
+/* the slab loop of tests/tp_01.cc:630-683 with TimeIntegratorHeat::solve /
+ * TimeIntegratorWave::solve (time_integrators.h:157-180,237-280);
+ * iterations: host array of n_slabs FGMRES counts (may be NULL) */
+STMG_API int stmg_solver_run(stmg_solver_t solver, int n_slabs, int *iterations, void *stream);
+/* copy the last slab's u (and v) blocks to host arrays of n_blocks x n_nodes */
+STMG_API int stmg_solver_solution(stmg_solver_t solver, double *u, double *v);
+/* SolverFGMRES::solve of the slab system (time_integrators.h:174) on device
+ * vectors x (initial guess in, solution out) and rhs */
+STMG_API int stmg_solver_solve(stmg_solver_t solver, double *x, const double *rhs, int *iterations, void *stream);
+/* GMG::vmult (gmg.h:846-859) on FP64 device vectors */
+STMG_API int stmg_gmg_vmult(stmg_solver_t solver, double *dst, const double *src, void *stream);
+/* the FP64 slab system SystemMatrix::vmult (operators.h:94-122) */
+STMG_API int stmg_solver_system_vmult(stmg_solver_t solver, double *dst, const double *src, void *stream);
 
 #ifdef __cplusplus
 }

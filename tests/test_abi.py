@@ -30,6 +30,7 @@ def test_bad_arguments_return_status_codes():
     assert L.stmg_mesh_create(4, n, 2, lo, hi, None, 0, None, C.byref(h)) == -1  # STMG_ERR_ARG
     assert b"dim" in L.stmg_last_error()
     assert L.stmg_mesh_create(3, n, 7, lo, hi, None, 0, None, C.byref(h)) == -8  # unsupported degree
+    assert L.stmg_mesh_create(3, n, 5, lo, hi, None, 0, None, C.byref(h)) == -8  # 3-D degree 5
     assert L.stmg_mesh_create(3, n, 2, lo, hi, None, 1, None, C.byref(h)) == -1  # coefficient missing
     assert L.stmg_op_vmult(None, None, None, None) == -2  # null handle
     assert L.stmg_mesh_destroy(None) == -2

@@ -1,0 +1,90 @@
+"""The slab solve on the GPU (FP64 FGMRES + FP32 space-time V-cycle) against
+the reference's golden 2-D runs (tests/tp_01.output: FGMRES totals per
+configuration) and against the CPU oracle (same iteration counts within one
+per slab, solution within 1e-7 relative)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import meshes
+import oracle_py as orc
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tp_01.json")
+
+
+def _gold():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+RECORD = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpurun_out", "tp01_gpu_iterations.jsonl")
+
+
+def _record(g, total):
+    """Appends GPU-vs-reference totals for the parity report (best effort)."""
+    try:
+        os.makedirs(os.path.dirname(RECORD), exist_ok=True)
+        with open(RECORD, "a") as f:
+            f.write(json.dumps(dict(section=g["section"], k=g["k"], refine=g["refine"], slabs=g["slabs"],
+                                    reference=g["iterations"], gpu=total)) + "\n")
+    except OSError:
+        pass
+
+
+GOLD_CASES = [g for g in _gold() if g["refine"] <= 4 and not (g["refine"] == 4 and g["k"] == 3)]
+
+
+@pytest.mark.parametrize("g", GOLD_CASES, ids=lambda g: f"{g['section']}-k{g['k']}-r{g['refine']}")
+def test_gpu_iterations_match_tp01(g):
+    import stmg
+    ttype = stmg.DG if g["type"] == "DG" else stmg.CGP
+    s = stmg.Solver(dim=2, refine=g["refine"], degree=g["k"] + 1, time_degree=g["k"], time_type=ttype,
+                    problem=stmg.HEAT if g["problem"] == "heat" else stmg.WAVE, n_steps=g["steps"],
+                    fe_degree_min=0 if ttype == stmg.DG else 1, n_steps_min=max(1, g["steps"] // 2))
+    assert s.n_nodes == g["s_dofs"]
+    its = s.run(g["slabs"])
+    total = int(its.sum())
+    _record(g, total)
+    # within one iteration per slab of the reference
+    assert abs(total - g["iterations"]) <= g["slabs"], (total, g["iterations"])
+
+
+@pytest.mark.parametrize("problem,ttype,k,steps", [("heat", "DG", 1, 1), ("heat", "CGP", 2, 1), ("wave", "DG", 1, 1),
+                                                   ("heat", "DG", 2, 2)])
+def test_gpu_solution_matches_oracle_2d(problem, ttype, k, steps):
+    import stmg
+    tt = stmg.DG if ttype == "DG" else stmg.CGP
+    pb = stmg.HEAT if problem == "heat" else stmg.WAVE
+    refine = 3
+    ref = orc.run(dim=2, refine=refine, p=k + 1, r=k, ttype=tt, problem=pb, n_steps=steps,
+                  fe_degree_min=0 if tt == stmg.DG else 1, n_steps_min=max(1, steps // 2), compute_errors=False)
+    s = stmg.Solver(dim=2, refine=refine, degree=k + 1, time_degree=k, time_type=tt, problem=pb, n_steps=steps,
+                    fe_degree_min=0 if tt == stmg.DG else 1, n_steps_min=max(1, steps // 2))
+    its = s.run(len(ref["iterations"]))
+    assert np.all(np.abs(its - ref["iterations"]) <= 1)
+    u, _ = s.solution()
+    assert np.linalg.norm(u - ref["u"]) <= 1e-7 * np.linalg.norm(ref["u"])
+
+
+def test_gpu_solution_matches_oracle_3d_coefficient():
+    """32^3-style heat slab with a log-uniform per-cell coefficient and a
+    nodal random source, scaled down to 4^3 Q2 cells, dG(1)."""
+    import stmg
+    dim, R = 3, 2
+    nf = (4, 4, 4)
+    coeff = meshes.log_uniform(64, 1e-1, 1e1, seed=3)
+    nn = 9 ** 3
+    f = np.random.default_rng(4).standard_normal(nn)
+    kw = dict(dim=3, refine=R, r=1, problem=orc.HEAT, n_steps=1, tau=1 / 8, n_slabs=3, rhs_mode=1)
+    ref = orc.run(p=2, ttype=orc.DG, f_nodal=f, fine_coeff=coeff, compute_errors=False, tol=1e-10, abs_tol=1e-14, **kw)
+    s = stmg.Solver(dim=3, refine=R, degree=2, time_degree=1, time_type=stmg.DG, problem=stmg.HEAT, n_steps=1,
+                    tau=1 / 8, rhs_mode=1, f_nodal=f, fine_coeff=coeff, tol=1e-10, abs_tol=1e-14)
+    its = s.run(3)
+    assert np.all(np.abs(its - ref["iterations"]) <= 1)
+    u, _ = s.solution()
+    assert np.linalg.norm(u - ref["u"]) <= 1e-7 * np.linalg.norm(ref["u"])
