@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark of the space-time multigrid slab solve on B200.
+
+Workload (one GPU): heat equation on the unit cube, 128^3 Q2 cells
+(257^3 = 16,974,593 nodes), dG(3) in time (4 time dofs, 67.9M space-time
+dofs per slab), 8 slabs of dt = 1/8, per-cell coefficient log-uniform in
+[0.1, 10] and a nodal source f_i ~ N(0,1), both seeded; each slab solved by
+FP64 FGMRES preconditioned with the FP32 space-time V-cycle (cell-patch
+Vanka, h/k transfers) to 1e-8 relative residual. A step is one slab solve.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+The JSON line carries the device-timed throughput (`value`), the end-to-end
+throughput through the C ABI with host buffers (`e2e`), the all-FP64
+V-cycle throughput on the same workload (`fp64_mg`), the roofline of the
+finest-level operator and Vanka kernels timed in isolation, the CPU oracle
+baseline on a bounded sample, clocks sampled during the timed region and the
+number of kernels launched.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "dealii-stfem_b200"))
+sys.path.insert(0, os.path.join(REPO, "tests"))
+
+METRIC = "space-time DoF/s to 1e-8 residual, FP32-MG vs FP64 on one B200; apply GB/s"
+SEED = 20261203
+
+
+def workload(refine=7):
+    n = 1 << refine
+    return dict(name=f"heat3d-{n}^3-Q2-dG3-8slabs", dim=3, refine=refine, degree=2, time_degree=3, n_steps=1,
+                tau=1.0 / 8, n_slabs=8, kappa=(0.1, 10.0), tol=1e-8, cells=n ** 3, nodes=(2 * n + 1) ** 3, nt=4)
+
+
+def inputs(w, seed=SEED):
+    rng = np.random.default_rng(seed)
+    kappa = 10.0 ** rng.uniform(np.log10(w["kappa"][0]), np.log10(w["kappa"][1]), size=w["cells"])
+    f = rng.standard_normal(w["nodes"])
+    return kappa, f
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------- CPU baseline
+def cpu_sample(w, seed=SEED, steps=1):
+    """The CPU oracle (one thread) on a bounded sample of the workload: the
+    same physics on 16^3 Q2 cells, dG(3), one slab per step."""
+    import oracle_py as orc
+    ws = workload(refine=4)
+    kappa, f = inputs(ws, seed)
+    t0 = time.perf_counter()
+    res = orc.run(dim=3, refine=ws["refine"], p=2, r=3, ttype=orc.DG, problem=orc.HEAT, n_steps=1, tau=ws["tau"],
+                  n_slabs=steps, rhs_mode=1, f_nodal=f, fine_coeff=kappa, compute_errors=False, tol=w["tol"],
+                  abs_tol=1e-300)
+    dt = time.perf_counter() - t0
+    dofs = ws["nodes"] * ws["nt"] * steps
+    return dict(value=dofs / dt, unit="DoF/s", cores=1, kind="port",
+                sample=f"oracle FP64 FGMRES + FP32 V-cycle, 16^3 Q2 cells dG(3), {steps} slab(s) incl. setup "
+                       f"({dt:.1f} s, {res['total_iterations']} FGMRES iterations)"), dt
+
+
+def run_reference(args):
+    """--impl reference: the oracle port of the reference's CPU path, timed on
+    the host (steps = slabs of the bounded sample; setup counted once)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle_py as orc
+    w = workload()
+    ws = workload(refine=4)
+    kappa, f = inputs(ws)
+    n = args.warmup + args.steps
+    t0 = time.perf_counter()
+    res = orc.run(dim=3, refine=ws["refine"], p=2, r=3, ttype=orc.DG, problem=orc.HEAT, n_steps=1, tau=ws["tau"],
+                  n_slabs=n, rhs_mode=1, f_nodal=f, fine_coeff=kappa, compute_errors=False, tol=w["tol"],
+                  abs_tol=1e-300)
+    dt = time.perf_counter() - t0
+    dofs = ws["nodes"] * ws["nt"] * n
+    value = dofs / dt
+    line = dict(metric=METRIC, value=value, unit="DoF/s", impl="reference", n_gpus=args.gpus, steps=args.steps,
+                warmup=args.warmup, ms_per_step=1e3 * dt / n, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f32", data="synthetic",
+                config=dict(workload=w["name"], sample="16^3 Q2 cells, dG(3), same seeded coefficient and source "
+                                                        "distributions", slabs=n),
+                cpu_baseline=dict(value=value, unit="DoF/s", cores=1, kind="port",
+                                  sample=f"{n} slabs of the 16^3 sample including setup"),
+                e2e=dict(value=value, unit="DoF/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+                fgmres_iterations=[int(i) for i in res["iterations"]])
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------- GPU arm
+def kernel_roofline(stmg, torch, w, kappa, hbm):
+    """Finest-level FP32 operator and Vanka apply timed in isolation with CUDA
+    events on the launching stream; algorithmic bytes per launch:
+      operator: 2 n_t N 4 (read src, write dst) + cells 4 (coefficient)
+      Vanka:    cells (nd^2 + nd) 4 (eigenvectors, eigenvalues) + 2 n_t N 4."""
+    n = 1 << w["refine"]
+    mesh = stmg.Mesh(3, (n, n, n), 2, coeff=kappa)
+    A, B, _, _, _ = stmg.time_weights(stmg.DG, 3, w["tau"], 1, stmg.HEAT)
+    N, nt = w["nodes"], w["nt"]
+    x = torch.randn(nt * N, device="cuda", dtype=torch.float32)
+    y = torch.empty_like(x)
+    s = torch.cuda.current_stream()
+    out = {}
+    op = stmg.Operator(mesh, A, B, dtype=stmg.F32)
+    vk = stmg.Vanka(mesh, A, B, compute=stmg.F32, storage=stmg.F32)
+    for name, fn, nbytes in (("st_apply", lambda: op.vmult(y, x), 2 * nt * N * 4 + w["cells"] * 4),
+                             ("vanka_apply", lambda: vk.vmult(y, x), w["cells"] * (27 * 27 + 27) * 4 + 2 * nt * N * 4)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        reps = 10
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        gbs = nbytes / t / 1e9
+        out[name] = dict(ms=t * 1e3, bytes=nbytes, achieved=gbs, frac=gbs / hbm)
+    del op, vk, mesh
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_ours(args):
+    import torch
+    import stmg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    w = workload(args.refine)
+    kappa, f = inputs(w, SEED + rank)
+    hbm, hbm_kind = peaks()
+
+    def make(mg_dtype):
+        return stmg.Solver(dim=3, refine=w["refine"], degree=2, time_degree=3, time_type=stmg.DG,
+                           problem=stmg.HEAT, n_steps=1, tau=w["tau"], mg_dtype=mg_dtype, tol=w["tol"],
+                           abs_tol=1e-300, rhs_mode=1, f_nodal=f, fine_coeff=kappa)
+
+    def timed(solver, steps, warmup):
+        solver.set_initial(np.zeros(w["nodes"]))
+        solver.run(warmup)
+        solver.set_initial(np.zeros(w["nodes"]))
+        s = torch.cuda.current_stream()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = stmg.kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        its = solver.run(steps)
+        e1.record(s)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        launches = stmg.kernel_launches() - l0
+        t = e0.elapsed_time(e1) / 1e3
+        if dist:
+            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t, its, launches
+
+    t_setup = time.perf_counter()
+    solver = make(stmg.F32)
+    t_setup = time.perf_counter() - t_setup
+    clocks = ClockSampler(local)
+    clocks.start()
+    t32, its32, launches = timed(solver, args.steps, args.warmup)
+    clk = clocks.stop()
+    dofs_step = w["nodes"] * w["nt"]
+    value = world * dofs_step * args.steps / t32
+
+    # end to end through the C ABI with host buffers: per step the slab's
+    # source goes host -> device (pinned) and the slab solution comes back
+    f_host = torch.from_numpy(f).pin_memory()
+    u_host = torch.empty(w["nt"] * w["nodes"], dtype=torch.float64).pin_memory()
+    solver.set_initial(np.zeros(w["nodes"]))
+    torch.cuda.synchronize()
+    te = time.perf_counter()
+    u_np = u_host.numpy()
+    for _ in range(args.steps):
+        solver.set_source(f_host.numpy())
+        solver.run(1)
+        solver.solution(u=u_np, want_v=False)
+    torch.cuda.synchronize()
+    te = time.perf_counter() - te
+    e2e = dict(value=world * dofs_step * args.steps / te, unit="DoF/s", h2d_bytes_per_step=w["nodes"] * 8,
+               d2h_bytes_per_step=w["nt"] * w["nodes"] * 8)
+    del solver
+    torch.cuda.empty_cache()
+
+    fp64 = None
+    if not args.no_fp64:
+        s64 = make(stmg.F64)
+        t64, its64, _ = timed(s64, args.steps, min(args.warmup, 1))
+        fp64 = dict(value=world * dofs_step * args.steps / t64, ms_per_step=1e3 * t64 / args.steps,
+                    fgmres_iterations=[int(i) for i in its64],
+                    speedup_fp32_mg=(world * dofs_step * args.steps / t32) / (world * dofs_step * args.steps / t64))
+        del s64
+        torch.cuda.empty_cache()
+
+    kr = kernel_roofline(stmg, torch, w, kappa, hbm)
+    dom = max(kr, key=lambda k: kr[k]["ms"])
+    roof = dict(kernel=dom, bound="hbm", achieved=kr[dom]["achieved"], peak=hbm, unit="GB/s",
+                frac=kr[dom]["frac"], traffic=None, peak_kind=hbm_kind,
+                kernels={k: dict(ms=v["ms"], algorithmic_bytes=v["bytes"], achieved_gbs=v["achieved"], frac=v["frac"])
+                         for k, v in kr.items()})
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu, _ = cpu_sample(w)
+
+    if rank == 0:
+        line = dict(metric=METRIC, value=value, unit="DoF/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
+                    ms_per_step=1e3 * t32 / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+                    dtype="f32", data="synthetic",
+                    config=dict(workload=w["name"], cells=w["cells"], nodes=w["nodes"], time_dofs=w["nt"],
+                                dofs_per_slab=dofs_step, outer="fgmres-fp64", mg="fp32 v-cycle, cell-patch vanka",
+                                tol=w["tol"], l2="inputs larger than L2 (FGMRES basis 30 x 0.54 GB)",
+                                parallelism="replicas" if world > 1 else "single-gpu", setup_s=t_setup),
+                    fgmres_iterations=[int(i) for i in its32], e2e=e2e, roofline=roof, cpu_baseline=cpu,
+                    clocks=clk, gpu_launches=int(launches), fp64_mg=fp64)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--refine", type=int, default=7, help="mesh 2^refine cells per direction (7: 128^3)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 V-cycle comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "solver.h"
+#include "time_fe.h"
 #include "st_operator.h"
 #include "stmg_internal.h"
 #include "transfer.h"
@@ -53,6 +54,11 @@ namespace stmg
   count_launch()
   {
     launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  void
+  add_launches(long long n)
+  {
+    launches.fetch_add(n, std::memory_order_relaxed);
   }
   long long
   launch_count()
@@ -115,6 +121,47 @@ extern "C"
     return guard([&] {
       STMG_REQUIRE(count, STMG_ERR_ARG, "kernel_launches: null argument");
       *count = launch_count();
+    });
+  }
+
+  int
+  stmg_time_weights(int time_type, int r, double tau, int n_steps, int problem, double *Alpha, double *Beta,
+                    double *rK, double *rM, double *rV)
+  {
+    return guard([&] {
+      STMG_REQUIRE(time_type == 1 || time_type == 2, STMG_ERR_ARG, "time_weights: time type 1 (cGP) or 2 (dG)");
+      STMG_REQUIRE(problem == 1 || problem == 2, STMG_ERR_ARG, "time_weights: problem 1 (heat) or 2 (wave)");
+      STMG_REQUIRE(r >= (time_type == 2 ? 0 : 1) && n_steps >= 1 && tau > 0, STMG_ERR_ARG, "time_weights: bad degree/steps");
+      STMG_REQUIRE(Alpha && Beta && rK && rM, STMG_ERR_ARG, "time_weights: null output");
+      const auto t  = tfe::Type(time_type);
+      auto       wn = tfe::slab_weights(t, r, tau, n_steps);
+      const int  nt = wn[0].m;
+      if (problem == 1)
+        {
+          std::copy(wn[0].a.begin(), wn[0].a.end(), Alpha);
+          std::copy(wn[1].a.begin(), wn[1].a.end(), Beta);
+          for (int i = 0; i < nt; ++i)
+            {
+              rK[i] = t == tfe::CGP ? wn[2](i, 0) : 0.0;
+              rM[i] = t == tfe::CGP ? wn[3](i, 0) : wn[2](i, 0);
+              if (rV)
+                rV[i] = 0.0;
+            }
+        }
+      else
+        {
+          auto w1 = tfe::slab_weights(t, r, tau, 1);
+          auto ww = tfe::wave_weights(t, w1[0], w1[1], w1[2], w1[3], n_steps);
+          std::copy(ww[0].a.begin(), ww[0].a.end(), Alpha);
+          std::copy(ww[1].a.begin(), ww[1].a.end(), Beta);
+          for (int i = 0; i < nt; ++i)
+            {
+              rK[i] = ww[2](i, 0);
+              rM[i] = ww[3](i, 0);
+              if (rV)
+                rV[i] = ww[4](i, 0);
+            }
+        }
     });
   }
 

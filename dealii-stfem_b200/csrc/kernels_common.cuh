@@ -6,6 +6,36 @@
 
 namespace stmg
 {
+  // Output combination of the cell-parallel kernels:
+  //   dst = rhs + alpha s + beta dst   (rhs optional, beta = 0 ignores dst)
+  // Constrained (Dirichlet) rows get rhs + beta dst.
+  template <typename T>
+  struct OutMode
+  {
+    T        alpha, beta;
+    const T *rhs;
+    __device__ __forceinline__ void
+    write(T *dst, long long i, T s) const
+    {
+      T v = alpha * s;
+      if (beta != T(0))
+        v += beta * dst[i];
+      if (rhs)
+        v += rhs[i];
+      dst[i] = v;
+    }
+    __device__ __forceinline__ void
+    write_constrained(T *dst, long long i) const
+    {
+      T v = T(0);
+      if (beta != T(0))
+        v += beta * dst[i];
+      if (rhs)
+        v += rhs[i];
+      dst[i] = v;
+    }
+  };
+
   template <int P1, int DIM>
   struct Tens
   {

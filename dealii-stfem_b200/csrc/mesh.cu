@@ -2,6 +2,9 @@
 // the cell tiling used by the cell-parallel kernels.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "stmg_internal.h"
 
@@ -126,5 +129,46 @@ namespace stmg
       }
     t.tile_stride = off;
     return t;
+  }
+
+  int
+  sm_count()
+  {
+    static int n = [] {
+      int dev = 0, c = 0;
+      STMG_CUDA(cudaGetDevice(&dev));
+      STMG_CUDA(cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev));
+      return c;
+    }();
+    return n;
+  }
+
+  unsigned
+  persistent_grid(const void *kernel, int block, std::size_t smem, long long work)
+  {
+    // the dynamic shared-memory limit is a per-kernel attribute: keep it at
+    // the largest size any caller needs
+    static std::mutex                                              mu;
+    static std::map<const void *, std::size_t>                     limit;
+    static std::map<std::pair<const void *, std::size_t>, int>     cache;
+    int                                                            per_sm = 0;
+    std::lock_guard<std::mutex>                                    lk(mu);
+    std::size_t                                                   &lim = limit[kernel];
+    if (smem > lim)
+      {
+        STMG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        lim = smem;
+      }
+    auto it = cache.find({kernel, smem});
+    if (it == cache.end())
+      {
+        STMG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem));
+        STMG_REQUIRE(per_sm > 0, STMG_ERR_UNSUPPORTED, "kernel does not fit on a multiprocessor");
+        cache[{kernel, smem}] = per_sm;
+      }
+    else
+      per_sm = it->second;
+    const long long g = std::min<long long>(work, (long long)per_sm * sm_count());
+    return unsigned(std::max<long long>(g, 1));
   }
 } // namespace stmg

@@ -1,6 +1,7 @@
 // Slab solve on the GPU (see solver.h).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "kernels_common.cuh"
@@ -258,6 +259,8 @@ namespace stmg
         lv.r_.alloc(bytes);
         lv.z.alloc(bytes);
       }
+    const char *ng = std::getenv("STMG_NO_GRAPH");
+    use_graph      = !(ng && ng[0] == '1');
     cudaStream_t s = nullptr;
     for (int l = 1; l < L; ++l)
       levels[l].omega = dtype == STMG_F64 ? estimate_relaxation<double>(l, s) : estimate_relaxation<float>(l, s);
@@ -286,12 +289,9 @@ namespace stmg
   void
   GMG::relax_step(int l, T *x, const T *b, cudaStream_t s)
   {
-    Level          &lv = levels[l];
-    const long long n  = lv.size();
-    lv.op->apply(false, x, as<T>(lv.r_), false, s);
-    sub_from<T>(n, b, as<T>(lv.r_), s);
-    lv.vanka->apply(as<T>(lv.r_), as<T>(lv.z), s);
-    axpby<T>(n, T(lv.omega), as<T>(lv.z), T(1), x, s);
+    Level &lv = levels[l];
+    lv.op->apply_ex(false, x, as<T>(lv.r_), -1.0, 0.0, b, s); // r = b - A x
+    lv.vanka->apply_ex(as<T>(lv.r_), x, lv.omega, 1.0, s);    // x += omega P r
   }
 
   // zero_start: MGSmootherPrecondition::apply (first sweep is
@@ -300,13 +300,11 @@ namespace stmg
   void
   GMG::smooth(int l, T *x, const T *b, bool zero_start, cudaStream_t s)
   {
-    Level          &lv = levels[l];
-    const long long n  = lv.size();
-    unsigned        k  = steps(l) * unsigned(cfg.smoothing_steps);
+    Level   &lv = levels[l];
+    unsigned k  = steps(l) * unsigned(cfg.smoothing_steps);
     if (zero_start)
       {
-        lv.vanka->apply(b, as<T>(lv.z), s);
-        axpby<T>(n, T(lv.omega), as<T>(lv.z), T(0), x, s);
+        lv.vanka->apply_ex(b, x, lv.omega, 0.0, s); // x = omega P b
         --k;
       }
     for (unsigned i = 0; i < k; ++i)
@@ -318,24 +316,60 @@ namespace stmg
   void
   GMG::vstep(int l, cudaStream_t s)
   {
-    Level          &lv = levels[l];
-    const long long n  = lv.size();
+    Level &lv = levels[l];
     if (l == 0)
       {
-        // MGCoarseGridApplySmoother: smooth from zero
-        fill<T>(n, T(0), as<T>(lv.sol), s);
-        smooth<T>(0, as<T>(lv.sol), as<T>(lv.def), false, s);
+        // MGCoarseGridApplySmoother: smooth from zero (its first sweep
+        // reduces to x = omega P b since A 0 = 0)
+        smooth<T>(0, as<T>(lv.sol), as<T>(lv.def), true, s);
         return;
       }
     smooth<T>(l, as<T>(lv.sol), as<T>(lv.def), true, s);
-    lv.op->apply(false, as<T>(lv.sol), as<T>(lv.t), false, s);
-    sub_from<T>(n, as<T>(lv.def), as<T>(lv.t), s);
+    lv.op->apply_ex(false, as<T>(lv.sol), as<T>(lv.t), -1.0, 0.0, as<T>(lv.def), s); // t = d - A x
     Level &co = levels[l - 1];
     fill<T>(co.size(), T(0), as<T>(co.def), s);
     lv.to_coarser->restrict_add(as<T>(lv.t), as<T>(co.def), s);
     vstep<T>(l - 1, s);
     lv.to_coarser->prolongate_add(as<T>(co.sol), as<T>(lv.sol), s);
     smooth<T>(l, as<T>(lv.sol), as<T>(lv.def), false, s);
+  }
+
+  // The V-cycle below the FP64/FP32 boundary works on the levels' own
+  // buffers only, so it is captured once into a CUDA graph and replayed.
+  template <typename T>
+  void
+  GMG::cycle(cudaStream_t s)
+  {
+    const int top = int(levels.size()) - 1;
+    if (!use_graph)
+      return vstep<T>(top, s);
+    if (!graph)
+      {
+        STMG_CUDA(cudaStreamSynchronize(s));
+        if (!cap)
+          STMG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        vstep<T>(top, cap); // warm-up: kernel attributes and occupancy caches
+        STMG_CUDA(cudaStreamSynchronize(cap));
+        const long long l0 = launch_count();
+        cudaGraph_t     g  = nullptr;
+        STMG_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        vstep<T>(top, cap);
+        STMG_CUDA(cudaStreamEndCapture(cap, &g));
+        graph_nodes = launch_count() - l0;
+        add_launches(-graph_nodes); // captured, not run
+        STMG_CUDA(cudaGraphInstantiate(&graph, g, 0));
+        STMG_CUDA(cudaGraphDestroy(g));
+      }
+    STMG_CUDA(cudaGraphLaunch(graph, s));
+    add_launches(graph_nodes);
+  }
+
+  GMG::~GMG()
+  {
+    if (graph)
+      cudaGraphExecDestroy(graph);
+    if (cap)
+      cudaStreamDestroy(cap);
   }
 
   void
@@ -346,13 +380,13 @@ namespace stmg
     if (dtype == STMG_F64)
       {
         convert<double, double>(n, src, as<double>(top.def), s);
-        vstep<double>(int(levels.size()) - 1, s);
+        cycle<double>(s);
         convert<double, double>(n, as<double>(top.sol), dst, s);
       }
     else
       {
         convert<float, double>(n, src, as<float>(top.def), s);
-        vstep<float>(int(levels.size()) - 1, s);
+        cycle<float>(s);
         convert<double, float>(n, as<float>(top.sol), dst, s);
       }
   }

@@ -49,6 +49,9 @@ namespace stmg
   {
   public:
     GMG(const SolverConfig &cfg, std::vector<std::unique_ptr<Mesh>> &meshes, Blas &blas);
+    ~GMG();
+    GMG(const GMG &)            = delete;
+    GMG &operator=(const GMG &) = delete;
     // FP64 in, FP64 out; FP32 or FP64 inside (GMG::vmult, gmg.h:846-859)
     void vmult(double *dst, const double *src, cudaStream_t s);
     std::vector<double> omegas() const;
@@ -57,6 +60,8 @@ namespace stmg
     std::vector<tfe::MG> seq;
 
   private:
+    template <typename T>
+    void cycle(cudaStream_t s);
     template <typename T>
     void vstep(int l, cudaStream_t s);
     template <typename T>
@@ -67,8 +72,12 @@ namespace stmg
     double estimate_relaxation(int l, cudaStream_t s);
     unsigned steps(int l) const;
 
-    SolverConfig cfg;
-    Blas        &blas;
+    SolverConfig    cfg;
+    Blas           &blas;
+    bool            use_graph = true;
+    cudaGraphExec_t graph     = nullptr;
+    cudaStream_t    cap       = nullptr;
+    long long       graph_nodes = 0;
   };
 
   // FGMRES(restart) with CGS2 orthogonalisation on device vectors.

@@ -18,8 +18,8 @@
 #include <algorithm>
 #include <cstring>
 
-#include "kernels_common.cuh"
 #include "st_operator.h"
+#include "tile_ops.cuh"
 
 namespace stmg
 {
@@ -155,130 +155,98 @@ namespace stmg
           out[q] = b[q];
     }
 
-    template <int DIM, int P, typename T, bool CART>
-    __global__ void __launch_bounds__(256)
+    template <int DIM, int P, typename T, bool CART, int TX, int TY, int TZ>
+    __global__ void __launch_bounds__(256, (sizeof(T) == 4 && CART) ? 2 : 1)
     st_apply_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<T> tm,
                     const __grid_constant__ Cart1D<T> c1, const __grid_constant__ QTab<T> qt,
-                    const T *__restrict__ src, T *__restrict__ dst, T *__restrict__ shell, int add)
+                    const T *__restrict__ src, T *__restrict__ dst, T *__restrict__ shell, const OutMode<T> om)
     {
-      constexpr int P1 = P + 1;
-      constexpr int ND = Tens<P1, DIM>::ND;
+      using S          = TileShape<DIM, P, TX, TY, TZ>;
+      constexpr int ND = S::ND;
       extern __shared__ __align__(16) unsigned char smem_raw[];
-      T *brick = reinterpret_cast<T *>(smem_raw);
-
-      int t[3], c0[3], tc[3], e[3];
-      tile_extents<DIM>(m, tl, blockIdx.x, t, c0, tc, e);
-      const int       nb      = e[0] * e[1] * e[2];
-      const int       nbmax   = tl.E[0] * tl.E[1] * tl.E[2];
-      T              *cellbuf = brick + (long long)tm.nt_in * nbmax;
-      const long long N       = m.N;
-
-      // A. brick of every input block
-      for (int idx = threadIdx.x; idx < tm.nt_in * nb; idx += blockDim.x)
+      const int nbuf    = max(tm.nt_in, tm.nt_out) * S::NB;
+      T        *bricks[2] = {reinterpret_cast<T *>(smem_raw), reinterpret_cast<T *>(smem_raw) + nbuf};
+      T        *cellbuf   = bricks[1] + nbuf;
+      long long tile      = blockIdx.x;
+      int       t[3], c0[3], tc[3], e[3];
+      if (tile < tl.n_tiles)
         {
-          const int i = idx / nb, r = idx % nb;
-          const int bx = r % e[0], by = (r / e[0]) % e[1], bz = r / (e[0] * e[1]);
-          const int gx = c0[0] * P + bx, gy = c0[1] * P + by, gz = c0[2] * P + bz;
-          T         v  = T(0);
-          if (!is_boundary_node(m, gx, gy, gz))
-            v = src[i * N + gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz)];
-          brick[i * nb + r] = v;
+          tile_extents<DIM>(m, tl, tile, t, c0, tc, e);
+          load_brick<S>(bricks[0], src, m, tm.nt_in, c0, e);
         }
-      __syncthreads();
-
-      // B. per (cell, output time dof)
-      const int ncell = tc[0] * tc[1] * tc[2];
-      for (int w = threadIdx.x; w < ncell * tm.nt_out; w += blockDim.x)
+      cp_async_commit();
+      for (int buf = 0; tile < tl.n_tiles; tile += gridDim.x, buf ^= 1)
         {
-          const int lc = w / tm.nt_out, j = w % tm.nt_out;
-          const int lx = lc % tc[0], ly = (lc / tc[0]) % tc[1], lz = lc / (tc[0] * tc[1]);
-          const int cx = c0[0] + lx, cy = c0[1] + ly, cz = c0[2] + lz;
-          const long long cell = cx + (long long)m.n[0] * (cy + (long long)m.n[1] * cz);
-          T kap = T(1);
-          if (CART && m.coeff_mode == 1)
-            kap = sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell]);
-          T a[ND], b[ND];
-#pragma unroll
-          for (int q = 0; q < ND; ++q)
-            a[q] = b[q] = T(0);
-          for (int i = 0; i < tm.nt_in; ++i)
+          tile_extents<DIM>(m, tl, tile, t, c0, tc, e);
+          const long long next = tile + gridDim.x;
+          if (next < tl.n_tiles)
             {
-              const T al = tm.A[j * tm.nt_in + i] * kap, be = tm.B[j * tm.nt_in + i];
-              if (al == T(0) && be == T(0))
+              int nt3[3], nc0[3], ntc[3], ne[3];
+              tile_extents<DIM>(m, tl, next, nt3, nc0, ntc, ne);
+              load_brick<S>(bricks[buf ^ 1], src, m, tm.nt_in, nc0, ne);
+            }
+          cp_async_commit();
+          cp_async_wait<1>();
+          __syncthreads();
+
+          // B. per (output time dof, cell): K a_j + M b_j into cellbuf
+          const T *brick = bricks[buf];
+          for (int w = threadIdx.x; w < tm.nt_out * S::TC; w += blockDim.x)
+            {
+              const int j = w / S::TC, lc = w - j * S::TC;
+              const int lx = lc % TX, ly = (lc / TX) % TY, lz = lc / (TX * TY);
+              if (lx >= tc[0] || ly >= tc[1] || lz >= tc[2])
                 continue;
-              const T *br = brick + i * nb + lx * P + e[0] * (ly * P + e[1] * (lz * P));
+              const int cx = c0[0] + lx, cy = c0[1] + ly, cz = c0[2] + lz;
+              const long long cell = cx + (long long)m.n[0] * (cy + (long long)m.n[1] * cz);
+              T kap = T(1);
+              if (CART && m.coeff_mode == 1)
+                kap = sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell]);
+              T a[ND], b[ND];
 #pragma unroll
               for (int q = 0; q < ND; ++q)
+                a[q] = b[q] = T(0);
+              const T *br0 = brick + lx * P + S::E0 * (ly * P + S::E1 * (lz * P));
+              for (int i = 0; i < tm.nt_in; ++i)
                 {
-                  const int qx = q % P1, qy = (q / P1) % P1, qz = q / (P1 * P1);
-                  const T   u  = br[qx + e[0] * (qy + e[1] * qz)];
-                  a[q] += al * u;
-                  b[q] += be * u;
-                }
-            }
-          T out[ND];
-          if constexpr (CART)
-            cart_apply<DIM, P>(c1, a, b, out);
-          else
-            general_apply<DIM, P>(m, qt, cx, cy, cz, cell, a, b, out);
-          T *cb = cellbuf + (long long)(lc * tm.nt_out + j) * ND;
+                  const T  al = tm.A[j * tm.nt_in + i] * kap, be = tm.B[j * tm.nt_in + i];
+                  const T *br = br0 + i * S::NB;
+                  if (al != T(0))
 #pragma unroll
-          for (int q = 0; q < ND; ++q)
-            cb[q] = out[q];
-        }
-      __syncthreads();
-
-      // C. gather per brick node and write
-      for (int idx = threadIdx.x; idx < tm.nt_out * nb; idx += blockDim.x)
-        {
-          const int j = idx / nb, r = idx % nb;
-          const int b3[3] = {r % e[0], (r / e[0]) % e[1], r / (e[0] * e[1])};
-          int       lc0[3], nlc[3];
+                    for (int q = 0; q < ND; ++q)
+                      a[q] += al * br[S::offset(q)];
+                  if (be != T(0))
 #pragma unroll
-          for (int d = 0; d < 3; ++d)
-            {
-              if (d >= DIM)
-                {
-                  lc0[d] = 0;
-                  nlc[d] = 1;
-                  continue;
+                    for (int q = 0; q < ND; ++q)
+                      b[q] += be * br[S::offset(q)];
                 }
-              const int q = b3[d] / P, rem = b3[d] % P;
-              if (rem == 0 && q > 0 && q < tc[d])
-                lc0[d] = q - 1, nlc[d] = 2;
+              T out[ND];
+              if constexpr (CART)
+                cart_apply<DIM, P>(c1, a, b, out);
               else
-                lc0[d] = min(q, tc[d] - 1), nlc[d] = 1;
+                general_apply<DIM, P>(m, qt, cx, cy, cz, cell, a, b, out);
+              T *cb = cellbuf + (j * S::TC + lc) * ND;
+#pragma unroll
+              for (int q = 0; q < ND; ++q)
+                cb[q] = out[q];
             }
-          T s = T(0);
-          for (int kz = 0; kz < nlc[2]; ++kz)
-            for (int ky = 0; ky < nlc[1]; ++ky)
-              for (int kx = 0; kx < nlc[0]; ++kx)
-                {
-                  const int cx = lc0[0] + kx, cy = lc0[1] + ky, cz = lc0[2] + kz;
-                  const int lc = cx + tc[0] * (cy + tc[1] * cz);
-                  const int ax = b3[0] - cx * P, ay = b3[1] - cy * P, az = DIM == 3 ? b3[2] - cz * P : 0;
-                  s += cellbuf[(long long)(lc * tm.nt_out + j) * ND + ax + P1 * (ay + P1 * az)];
-                }
-          bool interior = b3[0] > 0 && b3[0] < e[0] - 1 && b3[1] > 0 && b3[1] < e[1] - 1;
-          if (DIM == 3)
-            interior = interior && b3[2] > 0 && b3[2] < e[2] - 1;
-          if (interior)
-            {
-              const long long g = (c0[0] * P + b3[0]) + (long long)m.nn[0] * ((c0[1] * P + b3[1]) +
-                                                                                 (long long)m.nn[1] * (c0[2] * P + b3[2]));
-              T *d = dst + j * N + g;
-              *d   = add ? *d + s : s;
-            }
-          else
-            shell[((long long)blockIdx.x * tm.nt_out + j) * tl.tile_stride + shell_slot<DIM>(tl, e, b3[0], b3[1], b3[2])] = s;
+          __syncthreads();
+          // C. coloured scatter into the output brick (the current input
+          // brick's buffer, no longer read), D. write out
+          T *ob = bricks[buf];
+          scatter_cells<S, DIM, T>(cellbuf, ob, tm.nt_out, tc);
+          write_brick<S, DIM, T, false>(ob, m, tl, tile, tm.nt_out, c0, e, dst, shell, om);
+          __syncthreads();
         }
+      cp_async_wait<0>();
     }
 
     // Fix-up: nodes on tile boundaries (and Dirichlet nodes) get the sum of
     // their tiles' shell contributions in fixed order.
     template <int DIM, typename T>
     __global__ void
-    shell_fixup_kernel(const MeshView m, const Tiling tl, int nt, const T *__restrict__ shell, T *__restrict__ dst, int add)
+    shell_fixup_kernel(const MeshView m, const Tiling tl, int nt, const T *__restrict__ shell, T *__restrict__ dst,
+                       const OutMode<T> om)
     {
       const long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x;
       if (node >= m.N)
@@ -293,45 +261,70 @@ namespace stmg
         return;
       for (int j = 0; j < nt; ++j)
         {
-          T *d = dst + j * m.N + node;
+          const long long i = j * m.N + node;
           if (bd)
-            {
-              if (!add)
-                *d = T(0);
-              continue;
-            }
-          const T s = shell_sum<DIM, T>(m, tl, shell, nt, j, g);
-          *d        = add ? *d + s : s;
+            om.write_constrained(dst, i);
+          else
+            om.write(dst, i, shell_sum<DIM, T>(m, tl, shell, nt, j, g));
+        }
+    }
+
+    // compile-time tile shape per (dim, degree, precision); the fallback
+    // shape serves time dimensions whose bricks do not fit the main one
+    template <int DIM, int P, typename T, bool BIG>
+    struct OpShape
+    {
+      static constexpr int TX = DIM == 2 ? (P <= 2 ? (BIG ? 16 : 4) : (P <= 4 ? (BIG ? 8 : 2) : (BIG ? 4 : 1)))
+                                         : (P == 1 ? (BIG ? 8 : 2) : (P == 2 ? (BIG ? (sizeof(T) == 4 ? 8 : 4) : 2) : (BIG ? 4 : 1)));
+      static constexpr int TY = DIM == 2 ? TX : (P == 1 ? TX : (P == 2 ? (BIG ? 4 : 2) : (BIG ? (P == 3 ? 4 : 2) : 1)));
+      static constexpr int TZ = DIM == 2 ? 1 : (P == 1 ? TX : (P == 2 ? (BIG ? 4 : 2) : (BIG ? 2 : 1)));
+    };
+
+    template <int DIM, int P, typename T, bool BIG>
+    void
+    launch_shape(const StOperator &op, const TimeMats<T> &tm, const T *src, T *dst, T *shell, const OutMode<T> &om,
+                 const Tiling &tl, std::size_t smem, cudaStream_t s)
+    {
+      using Sh = OpShape<DIM, P, T, BIG>;
+      const MeshView &m    = op.mesh->v;
+      auto            kern = m.cartesian ? st_apply_kernel<DIM, P, T, true, Sh::TX, Sh::TY, Sh::TZ>
+                                         : st_apply_kernel<DIM, P, T, false, Sh::TX, Sh::TY, Sh::TZ>;
+      const unsigned  grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, tl.n_tiles);
+      kern<<<grid, 256, smem, s>>>(m, tl, tm, op.cart<T>(), op.qtab<T>(), src, dst, shell, om);
+      count_launch();
+      STMG_CUDA(cudaGetLastError());
+      if (tl.n_tiles > 1)
+        {
+          const unsigned nb = unsigned((m.N + 255) / 256);
+          shell_fixup_kernel<DIM, T><<<nb, 256, 0, s>>>(m, tl, tm.nt_out, shell, dst, om);
+          count_launch();
+          STMG_CUDA(cudaGetLastError());
         }
     }
 
     template <int DIM, int P, typename T>
     void
-    launch_dp(const StOperator &op, bool transpose, const T *src, T *dst, T *shell, bool add, cudaStream_t s)
+    launch_dp(const StOperator &op, bool transpose, const T *src, T *dst, T *shell, const OutMode<T> &om,
+              cudaStream_t s)
     {
-      const TimeMats<T> &tm   = transpose ? op.tmT<T>() : op.tm<T>();
-      const MeshView    &m    = op.mesh->v;
-      const Tiling      &tl   = transpose ? op.tilingT : op.tiling;
-      const std::size_t  smem = op.smem_bytes(tl, tm.nt_in, tm.nt_out, sizeof(T));
-      auto               kern = m.cartesian ? st_apply_kernel<DIM, P, T, true> : st_apply_kernel<DIM, P, T, false>;
-      STMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      kern<<<unsigned(tl.n_tiles), 256, smem, s>>>(m, tl, tm, op.cart<T>(), op.qtab<T>(), src, dst, shell, add ? 1 : 0);
-      count_launch();
-      STMG_CUDA(cudaGetLastError());
-      const unsigned nb = unsigned((m.N + 255) / 256);
-      shell_fixup_kernel<DIM, T><<<nb, 256, 0, s>>>(m, tl, tm.nt_out, shell, dst, add ? 1 : 0);
-      count_launch();
-      STMG_CUDA(cudaGetLastError());
+      const TimeMats<T> &tm  = transpose ? op.tmT<T>() : op.tm<T>();
+      const bool         big = transpose ? op.bigT : op.big;
+      const Tiling      &tl  = transpose ? op.tilingT : op.tiling;
+      const std::size_t  smem = op.smem_bytes(transpose ? op.shpT : op.shp, tm.nt_in, tm.nt_out, sizeof(T));
+      if (big)
+        launch_shape<DIM, P, T, true>(op, tm, src, dst, shell, om, tl, smem, s);
+      else
+        launch_shape<DIM, P, T, false>(op, tm, src, dst, shell, om, tl, smem, s);
     }
 
     template <typename T>
     void
-    launch(const StOperator &op, bool transpose, const T *src, T *dst, T *shell, bool add, cudaStream_t s)
+    launch(const StOperator &op, bool transpose, const T *src, T *dst, T *shell, const OutMode<T> &om, cudaStream_t s)
     {
       const int dim = op.mesh->v.dim, p = op.mesh->v.p;
 #define STMG_CASE(D, PP)                                                                                 \
   if (dim == D && p == PP)                                                                               \
-    return launch_dp<D, PP, T>(op, transpose, src, dst, shell, add, s);
+    return launch_dp<D, PP, T>(op, transpose, src, dst, shell, om, s);
       STMG_CASE(2, 1) STMG_CASE(2, 2) STMG_CASE(2, 3) STMG_CASE(2, 4) STMG_CASE(2, 5)
       STMG_CASE(3, 1) STMG_CASE(3, 2) STMG_CASE(3, 3) STMG_CASE(3, 4)
 #undef STMG_CASE
@@ -373,28 +366,58 @@ namespace stmg
     }
   } // namespace
 
-  std::size_t
-  StOperator::smem_bytes(const Tiling &tl, int nt_in_, int nt_out_, std::size_t elem) const
+  namespace
   {
-    const int nd = mesh->nd;
-    return elem * (std::size_t(nt_in_) * tl.E[0] * tl.E[1] * tl.E[2] +
-                   std::size_t(tl.T[0]) * tl.T[1] * tl.T[2] * nt_out_ * nd);
+    template <typename T>
+    void
+    shape_of(int dim, int p, bool big, int *T3)
+    {
+#define STMG_SH(D, PP)                                                                                   \
+  if (dim == D && p == PP)                                                                               \
+    {                                                                                                    \
+      if (big)                                                                                           \
+        T3[0] = OpShape<D, PP, T, true>::TX, T3[1] = OpShape<D, PP, T, true>::TY, T3[2] = OpShape<D, PP, T, true>::TZ; \
+      else                                                                                               \
+        T3[0] = OpShape<D, PP, T, false>::TX, T3[1] = OpShape<D, PP, T, false>::TY, T3[2] = OpShape<D, PP, T, false>::TZ; \
+      return;                                                                                            \
+    }
+      STMG_SH(2, 1) STMG_SH(2, 2) STMG_SH(2, 3) STMG_SH(2, 4) STMG_SH(2, 5)
+      STMG_SH(3, 1) STMG_SH(3, 2) STMG_SH(3, 3) STMG_SH(3, 4)
+#undef STMG_SH
+      throw Error(STMG_ERR_UNSUPPORTED, "operator: unsupported dim/degree");
+    }
+  } // namespace
+
+  std::size_t
+  StOperator::smem_bytes(const int *shape, int nt_in_, int nt_out_, std::size_t elem) const
+  {
+    // two bricks (each holding the larger of the input and output blocks)
+    // and the per-cell results, for the compile-time tile shape
+    const int         p = mesh->v.p, dim = mesh->v.dim;
+    const std::size_t nb = std::size_t(shape[0] * p + 1) * (shape[1] * p + 1) * (dim == 3 ? shape[2] * p + 1 : 1);
+    const std::size_t tc = std::size_t(shape[0]) * shape[1] * (dim == 3 ? shape[2] : 1);
+    return elem * (2 * std::size_t(std::max(nt_in_, nt_out_)) * nb + tc * nt_out_ * mesh->nd);
   }
 
   Tiling
-  StOperator::choose_tiling(int nt_in_, int nt_out_) const
+  StOperator::choose_tiling(int nt_in_, int nt_out_, bool &big_out, int *shape) const
   {
-    const MeshView  &m     = mesh->v;
-    const std::size_t elem = dtype == STMG_F64 ? 8 : 4;
-    const std::size_t budget = 100 * 1024;
-    static const int cand3[][3] = {{8, 8, 4}, {8, 4, 4}, {4, 4, 4}, {4, 4, 2}, {4, 2, 2}, {2, 2, 2}, {2, 2, 1}, {2, 1, 1}, {1, 1, 1}};
-    static const int cand2[][3] = {{16, 16, 1}, {16, 8, 1}, {8, 8, 1}, {8, 4, 1}, {4, 4, 1}, {4, 2, 1}, {2, 2, 1}, {2, 1, 1}, {1, 1, 1}};
-    const int(*cand)[3] = m.dim == 3 ? cand3 : cand2;
-    for (int k = 0; k < 9; ++k)
+    const std::size_t elem   = dtype == STMG_F64 ? 8 : 4;
+    const std::size_t budget = 200 * 1024;
+    for (bool big : {true, false})
       {
-        Tiling t = make_tiling(m, cand[k]);
-        if (smem_bytes(t, nt_in_, nt_out_, elem) <= budget)
-          return t;
+        int T3[3];
+        if (dtype == STMG_F64)
+          shape_of<double>(mesh->v.dim, mesh->v.p, big, T3);
+        else
+          shape_of<float>(mesh->v.dim, mesh->v.p, big, T3);
+        if (smem_bytes(T3, nt_in_, nt_out_, elem) <= budget)
+          {
+            big_out = big;
+            for (int d = 0; d < 3; ++d)
+              shape[d] = T3[d];
+            return make_tiling(mesh->v, T3);
+          }
       }
     throw Error(STMG_ERR_UNSUPPORTED, "operator: time blocks do not fit in shared memory");
   }
@@ -418,8 +441,8 @@ namespace stmg
     cart32 = make_cart<float>(mesh->v);
     qtab64 = make_qtab<double>(mesh->v.p);
     qtab32 = make_qtab<float>(mesh->v.p);
-    tiling  = choose_tiling(nt_in, nt_out);
-    tilingT = choose_tiling(nt_out, nt_in);
+    tiling  = choose_tiling(nt_in, nt_out, big, shp);
+    tilingT = choose_tiling(nt_out, nt_in, bigT, shpT);
     const std::size_t elem = dtype == STMG_F64 ? 8 : 4;
     const std::size_t n1   = std::size_t(tiling.n_tiles) * nt_out * tiling.tile_stride;
     const std::size_t n2   = std::size_t(tilingT.n_tiles) * nt_in * tilingT.tile_stride;
@@ -429,12 +452,25 @@ namespace stmg
   void
   StOperator::apply(bool transpose, const void *src, void *dst, bool add, cudaStream_t s) const
   {
+    apply_ex(transpose, src, dst, 1.0, add ? 1.0 : 0.0, nullptr, s);
+  }
+
+  void
+  StOperator::apply_ex(bool transpose, const void *src, void *dst, double alpha, double beta, const void *rhs,
+                       cudaStream_t s) const
+  {
     STMG_REQUIRE(src && dst, STMG_ERR_ARG, "operator: null vector");
     if (dtype == STMG_F64)
-      launch<double>(*this, transpose, static_cast<const double *>(src), static_cast<double *>(dst),
-                     reinterpret_cast<double *>(shell.ptr), add, s);
+      {
+        const OutMode<double> om{alpha, beta, static_cast<const double *>(rhs)};
+        launch<double>(*this, transpose, static_cast<const double *>(src), static_cast<double *>(dst),
+                       reinterpret_cast<double *>(shell.ptr), om, s);
+      }
     else
-      launch<float>(*this, transpose, static_cast<const float *>(src), static_cast<float *>(dst),
-                    reinterpret_cast<float *>(shell.ptr), add, s);
+      {
+        const OutMode<float> om{float(alpha), float(beta), static_cast<const float *>(rhs)};
+        launch<float>(*this, transpose, static_cast<const float *>(src), static_cast<float *>(dst),
+                      reinterpret_cast<float *>(shell.ptr), om, s);
+      }
   }
 } // namespace stmg

@@ -13,11 +13,17 @@ namespace stmg
 
     // dst (+)= op(src) (transpose: A^T, B^T) on stream s
     void apply(bool transpose, const void *src, void *dst, bool add, cudaStream_t s) const;
+    // dst = rhs + alpha op(src) + beta dst (rhs may be null): the residual
+    // b - A x is alpha = -1, beta = 0
+    void apply_ex(bool transpose, const void *src, void *dst, double alpha, double beta, const void *rhs,
+                  cudaStream_t s) const;
 
     Mesh               *mesh;
     int                 nt_out, nt_in, dtype;
     std::vector<double> A, B;
     Tiling              tiling, tilingT;
+    bool                big = true, bigT = true; // compile-time tile shape in use
+    int                 shp[3] = {1, 1, 1}, shpT[3] = {1, 1, 1};
 
     template <typename T>
     const TimeMats<T> &tm() const
@@ -51,10 +57,10 @@ namespace stmg
       else
         return qtab32;
     }
-    std::size_t smem_bytes(const Tiling &tl, int nt_in, int nt_out, std::size_t elem) const;
+    std::size_t smem_bytes(const int *shape, int nt_in, int nt_out, std::size_t elem) const;
 
   private:
-    Tiling choose_tiling(int nt_in, int nt_out) const;
+    Tiling choose_tiling(int nt_in, int nt_out, bool &big, int *shape) const;
 
     TimeMats<double> tm64, tmT64;
     TimeMats<float>  tm32, tmT32;

@@ -31,6 +31,7 @@ namespace stmg
 
   // Number of kernels this library has launched (diagnostic counter).
   void      count_launch();
+  void      add_launches(long long n);
   long long launch_count();
 
 #define STMG_CUDA(call)                                                                                  \
@@ -183,6 +184,12 @@ namespace stmg
     long long n_tiles;
   };
   Tiling make_tiling(const MeshView &m, const int *T);
+
+  // Grid of a persistent kernel: as many CTAs as fit on the device at once
+  // (occupancy with the given block size and dynamic shared memory), at most
+  // `work` CTAs. Also raises the kernel's dynamic shared-memory limit.
+  unsigned persistent_grid(const void *kernel, int block, std::size_t smem, long long work);
+  int      sm_count();
 
   // Time coupling matrices of an operator (kernel parameter).
   template <typename T>

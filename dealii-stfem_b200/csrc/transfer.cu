@@ -29,8 +29,7 @@ namespace stmg
       const int g[3] = {int(node % fm.nn[0]), int((node / fm.nn[0]) % fm.nn[1]), int(node / ((long long)fm.nn[0] * fm.nn[1]))};
       if (is_boundary_node(fm, g[0], g[1], g[2]))
         return;
-      const int p1 = fm.p + 1, stride_d = 3 * 0 + 1;
-      (void)stride_d;
+      const int p1 = fm.p + 1;
       // 1-D stencils: coarse nodes start[d][g_d] .. +p with weights
       int    s[3], cnt[3];
       const double *wd[3];
@@ -227,11 +226,10 @@ namespace stmg
     if (dtype == STMG_F64)
       h_prolongate_kernel<double><<<nb, 256, 0, s>>>(f, c, nt, p_start.ptr, p_w.ptr, static_cast<const double *>(src),
                                                      static_cast<double *>(dst));
-      count_launch();
     else
       h_prolongate_kernel<float><<<nb, 256, 0, s>>>(f, c, nt, p_start.ptr, p_w.ptr, static_cast<const float *>(src),
                                                     static_cast<float *>(dst));
-      count_launch();
+    count_launch();
     STMG_CUDA(cudaGetLastError());
   }
 
@@ -243,11 +241,10 @@ namespace stmg
     if (dtype == STMG_F64)
       h_restrict_kernel<double><<<nb, 256, 0, s>>>(f, c, nt, maxr, r_cnt.ptr, r_f.ptr, r_w.ptr,
                                                    static_cast<const double *>(src), static_cast<double *>(dst));
-      count_launch();
     else
       h_restrict_kernel<float><<<nb, 256, 0, s>>>(f, c, nt, maxr, r_cnt.ptr, r_f.ptr, r_w.ptr,
                                                   static_cast<const float *>(src), static_cast<float *>(dst));
-      count_launch();
+    count_launch();
     STMG_CUDA(cudaGetLastError());
   }
 
@@ -283,11 +280,10 @@ namespace stmg
     if (dtype == STMG_F64)
       time_transfer_kernel<double><<<nb, 256, 0, s>>>(N, nt_fine, nt_coarse, P64, static_cast<const double *>(src),
                                                       static_cast<double *>(dst));
-      count_launch();
     else
       time_transfer_kernel<float><<<nb, 256, 0, s>>>(N, nt_fine, nt_coarse, P32, static_cast<const float *>(src),
                                                      static_cast<float *>(dst));
-      count_launch();
+    count_launch();
     STMG_CUDA(cudaGetLastError());
   }
 
@@ -299,11 +295,10 @@ namespace stmg
     if (dtype == STMG_F64)
       time_transfer_kernel<double><<<nb, 256, 0, s>>>(N, nt_coarse, nt_fine, R64, static_cast<const double *>(src),
                                                       static_cast<double *>(dst));
-      count_launch();
     else
       time_transfer_kernel<float><<<nb, 256, 0, s>>>(N, nt_coarse, nt_fine, R32, static_cast<const float *>(src),
                                                      static_cast<float *>(dst));
-      count_launch();
+    count_launch();
     STMG_CUDA(cudaGetLastError());
   }
 } // namespace stmg

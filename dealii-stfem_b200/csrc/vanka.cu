@@ -21,6 +21,7 @@
 
 #include "kernels_common.cuh"
 #include "vanka.h"
+#include "vanka_apply_impl.cuh"
 
 namespace stmg
 {
@@ -50,8 +51,9 @@ namespace stmg
     template <int DIM, int P, bool CART, typename TS>
     __global__ void
     vanka_setup_kernel(const MeshView m, const double *__restrict__ Kref, const double *__restrict__ Mref,
-                       const double *__restrict__ elemK, const double *__restrict__ elemM, TS *__restrict__ Vout,
-                       double *__restrict__ mu_out, int *__restrict__ status)
+                       const double *__restrict__ elemK, const double *__restrict__ elemM,
+                       unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int mu_double,
+                       int *__restrict__ status)
     {
       constexpr int P1 = P + 1;
       constexpr int ND = Tens<P1, DIM>::ND;
@@ -275,13 +277,17 @@ namespace stmg
                 s -= M[k][i] * Q[k][col];
               Q[i][col] = s / M[i][i];
             }
-          mu_out[cell * ND + col] = K[col][col];
+          unsigned char *mr = rec + cell * rec_bytes + mu_off;
+          if (mu_double)
+            reinterpret_cast<double *>(mr)[col] = K[col][col];
+          else
+            reinterpret_cast<float *>(mr)[col] = float(K[col][col]);
         }
       __syncthreads();
       for (int e = tid; e < ND * ND; e += nth)
         {
           const int mm = e / ND, a = e % ND;
-          Vout[cell * ND * ND + e] = to_storage<TS>(Q[a][mm]);
+          reinterpret_cast<TS *>(rec + cell * rec_bytes)[e] = to_storage<TS>(Q[a][mm]);
         }
     }
 
@@ -365,10 +371,14 @@ namespace stmg
 
   // ------------------------------------------------------------------ host
   std::size_t
-  Vanka::smem_bytes(const Tiling &tl) const
+  Vanka::smem_bytes(const int *T3) const
   {
     const std::size_t elem = compute == STMG_F64 ? 8 : 4;
-    return elem * (std::size_t(nt) * tl.E[0] * tl.E[1] * tl.E[2] + 2ull * tl.T[0] * tl.T[1] * tl.T[2] * nt * mesh->nd);
+    const int         p = mesh->v.p, dim = mesh->v.dim;
+    const std::size_t nb = std::size_t(T3[0] * p + 1) * (T3[1] * p + 1) * (dim == 3 ? T3[2] * p + 1 : 1);
+    const std::size_t tc = std::size_t(T3[0]) * T3[1] * (dim == 3 ? T3[2] : 1);
+    return 2ull * chunk * rec_bytes +
+           elem * (2ull * nt * nb + std::size_t(chunk) * nt * mesh->nd + tc * nt * mesh->nd);
   }
 
   namespace
@@ -381,7 +391,7 @@ namespace stmg
       const MeshView &m  = vk.mesh->v;
       DevBuf<int>     status(1);
       STMG_CUDA(cudaMemset(status.ptr, 0, sizeof(int)));
-      DevBuf<double> Kref, Mref, eK, eM, mu64(m.ncells * ND);
+      DevBuf<double> Kref, Mref, eK, eM;
       const int      threads = ND <= 32 ? 32 : 64;
       if (m.cartesian)
         {
@@ -422,7 +432,9 @@ namespace stmg
         using TS  = std::remove_pointer_t<decltype(Vp)>;
         auto kern = m.cartesian ? vanka_setup_kernel<DIM, P, true, TS> : vanka_setup_kernel<DIM, P, false, TS>;
         STMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        kern<<<unsigned(m.ncells), threads, smem>>>(m, Kref.ptr, Mref.ptr, eK.ptr, eM.ptr, Vp, mu64.ptr, status.ptr);
+        (void)Vp;
+        kern<<<unsigned(m.ncells), threads, smem>>>(m, Kref.ptr, Mref.ptr, eK.ptr, eM.ptr, vk.V.ptr, vk.rec_bytes,
+                                                    vk.mu_off, vk.compute == STMG_F64 ? 1 : 0, status.ptr);
         count_launch();
         STMG_CUDA(cudaGetLastError());
       };
@@ -436,19 +448,6 @@ namespace stmg
       int st = 0;
       STMG_CUDA(cudaMemcpy(&st, status.ptr, sizeof(int), cudaMemcpyDeviceToHost));
       STMG_REQUIRE(st == 0, STMG_ERR_NONFINITE, "vanka setup: patch mass matrix not positive definite");
-      if (vk.compute == STMG_F64)
-        {
-          vk.mu.alloc(m.ncells * ND * 8);
-          STMG_CUDA(cudaMemcpy(vk.mu.ptr, mu64.ptr, m.ncells * ND * 8, cudaMemcpyDeviceToDevice));
-        }
-      else
-        {
-          std::vector<double> h(m.ncells * ND);
-          STMG_CUDA(cudaMemcpy(h.data(), mu64.ptr, h.size() * 8, cudaMemcpyDeviceToHost));
-          std::vector<float> f(h.begin(), h.end());
-          vk.mu.alloc(f.size() * 4);
-          STMG_CUDA(cudaMemcpy(vk.mu.ptr, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
-        }
     }
 
   } // namespace
@@ -477,21 +476,34 @@ namespace stmg
       }
     const std::size_t nd   = mesh->nd;
     const std::size_t elem = storage == STMG_F64 ? 8 : (storage == STMG_F32 ? 4 : 2);
-    V.alloc(std::size_t(mesh->v.ncells) * nd * nd * elem);
+    auto              pad  = [](std::size_t b) { return (b + 15) / 16 * 16; };
+    mu_off                 = int(pad(nd * nd * elem));
+    rec_bytes              = int(pad(mu_off + nd * (compute == STMG_F64 ? 8 : 4)));
+    V.alloc(std::size_t(mesh->v.ncells) * rec_bytes);
 #define STMG_SETUP(D, PP)                                                                                \
   if (dim == D && p == PP)                                                                               \
     run_setup<D, PP>(*this);
     STMG_SETUP(2, 1) STMG_SETUP(2, 2) STMG_SETUP(2, 3) STMG_SETUP(2, 4) STMG_SETUP(2, 5)
     STMG_SETUP(3, 1) STMG_SETUP(3, 2) STMG_SETUP(3, 3)
 #undef STMG_SETUP
-    // tiling within a shared-memory budget
-    static const int cand3[][3] = {{8, 4, 4}, {4, 4, 4}, {4, 4, 2}, {4, 2, 2}, {2, 2, 2}, {2, 2, 1}, {2, 1, 1}, {1, 1, 1}};
-    static const int cand2[][3] = {{16, 8, 1}, {8, 8, 1}, {8, 4, 1}, {4, 4, 1}, {4, 2, 1}, {2, 2, 1}, {2, 1, 1}, {1, 1, 1}};
+    // compile-time tile shape and record chunk within a shared-memory budget
     bool ok = false;
-    for (int k = 0; k < 8 && !ok; ++k)
+    for (bool b : {true, false})
       {
-        tiling = make_tiling(mesh->v, dim == 3 ? cand3[k] : cand2[k]);
-        ok     = smem_bytes(tiling) <= 100 * 1024;
+        if (ok)
+          break;
+        vanka_shape(dim, p, b, shape);
+        for (int ch : {8, 4, 2, 1})
+          {
+            chunk = ch;
+            if (smem_bytes(shape) <= (b ? 112 : 200) * 1024)
+              {
+                ok     = true;
+                big    = b;
+                tiling = make_tiling(mesh->v, shape);
+                break;
+              }
+          }
       }
     STMG_REQUIRE(ok, STMG_ERR_UNSUPPORTED, "vanka: does not fit in shared memory");
     shell.alloc(std::size_t(tiling.n_tiles) * nt * tiling.tile_stride * (compute == STMG_F64 ? 8 : 4));
@@ -500,11 +512,15 @@ namespace stmg
   void
   Vanka::apply(const void *src, void *dst, cudaStream_t s) const
   {
+    apply_ex(src, dst, 1.0, 0.0, s);
+  }
+
+  void
+  Vanka::apply_ex(const void *src, void *dst, double alpha, double beta, cudaStream_t s) const
+  {
     STMG_REQUIRE(src && dst, STMG_ERR_ARG, "vanka: null vector");
-    const int dim = mesh->v.dim, p = mesh->v.p;
-    (void)p;
-    if (dim == 2)
-      return vanka_apply_2d(*this, src, dst, s);
-    return vanka_apply_3d(*this, src, dst, s);
+    if (mesh->v.dim == 2)
+      return vanka_apply_2d(*this, src, dst, alpha, beta, s);
+    return vanka_apply_3d(*this, src, dst, alpha, beta, s);
   }
 } // namespace stmg

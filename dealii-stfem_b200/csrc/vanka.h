@@ -15,8 +15,11 @@ namespace stmg
 
     // dst = sum_c R_c^T diag(1/valence) B_c^{-1} R_c src (dst overwritten)
     void apply(const void *src, void *dst, cudaStream_t s) const;
+    // dst = alpha P src + beta dst (the relaxation update x += omega P r is
+    // alpha = omega, beta = 1)
+    void apply_ex(const void *src, void *dst, double alpha, double beta, cudaStream_t s) const;
 
-    std::size_t smem_bytes(const Tiling &tl) const;
+    std::size_t smem_bytes(const int *shape) const;
     template <typename T>
     const TimeMats<T> &tmats() const
     {
@@ -25,18 +28,22 @@ namespace stmg
       else
         return tm32;
     }
-    std::size_t inverse_bytes() const { return V.n + mu.n; }
+    std::size_t inverse_bytes() const { return V.n; }
 
     Mesh                 *mesh;
     int                   nt, compute, storage;
     Tiling                tiling;
-    DevBuf<unsigned char> V;     // per cell, V as [mode][dof] in the storage type
-    DevBuf<unsigned char> mu;    // per cell eigenvalues in the compute type
+    // per cell one record: V as [mode][dof] in the storage type, padded to
+    // 16 bytes, then the eigenvalues mu in the compute type, padded to 16 bytes
+    DevBuf<unsigned char> V;
+    int                   rec_bytes = 0, mu_off = 0, chunk = 8;
+    bool                  big = true;                // compile-time tile shape in use
+    int                   shape[3] = {1, 1, 1};
     DevBuf<unsigned char> shell; // tile face slots (scratch)
     TimeMats<double>      tm64;
     TimeMats<float>       tm32;
   };
 
-  void vanka_apply_2d(const Vanka &vk, const void *src, void *dst, cudaStream_t s);
-  void vanka_apply_3d(const Vanka &vk, const void *src, void *dst, cudaStream_t s);
+  void vanka_apply_2d(const Vanka &vk, const void *src, void *dst, double alpha, double beta, cudaStream_t s);
+  void vanka_apply_3d(const Vanka &vk, const void *src, void *dst, double alpha, double beta, cudaStream_t s);
 } // namespace stmg

@@ -4,7 +4,7 @@
 
 #include <cuda_bf16.h>
 
-#include "kernels_common.cuh"
+#include "tile_ops.cuh"
 #include "vanka.h"
 
 namespace stmg
@@ -100,156 +100,168 @@ namespace stmg
       return v;
     }
 
-    template <int DIM, int P, typename T, typename TS, int NT>
-    __global__ void __launch_bounds__(256)
+    // Per cell the setup stores one record: V as [mode][dof] in the storage
+    // type, padded to 16 bytes, then mu (nd values of the compute type),
+    // padded to 16 bytes; rec_bytes = record stride. Records stream through
+    // shared memory in chunks of `chunk` cells (cp.async, double buffered).
+    template <int DIM, int P, typename T, typename TS, int NT, int TX, int TY, int TZ>
+    __global__ void __launch_bounds__(256, 2)
     vanka_apply_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<T> tm,
-                       const TS *__restrict__ V, const T *__restrict__ mu, const T *__restrict__ src,
-                       T *__restrict__ dst, T *__restrict__ shell)
+                       const unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int chunk,
+                       const T *__restrict__ src, T *__restrict__ dst, T *__restrict__ shell, const OutMode<T> om)
     {
-      constexpr int P1 = P + 1;
-      constexpr int ND = Tens<P1, DIM>::ND;
+      using S          = TileShape<DIM, P, TX, TY, TZ>;
+      constexpr int ND = S::ND;
       constexpr int NA = NT > 0 ? NT : MAX_NT;
       extern __shared__ __align__(16) unsigned char vk_smem[];
-      T        *brick = reinterpret_cast<T *>(vk_smem);
-      const int nt    = tm.nt_out;
+      const int      nt      = tm.nt_out;
+      unsigned char *recs[2] = {vk_smem, vk_smem + (long long)chunk * rec_bytes};
+      T             *bricks[2];
+      bricks[0]     = reinterpret_cast<T *>(vk_smem + 2ll * chunk * rec_bytes);
+      bricks[1]     = bricks[0] + nt * S::NB;
+      T *zbuf       = bricks[1] + nt * S::NB;
+      T *obuf       = zbuf + chunk * nt * ND;
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+      const int r16  = rec_bytes / 16;
+      const int nch  = (S::TC + chunk - 1) / chunk;
 
+      auto issue = [&](long long tl_i, int chk, int rb, int bb) {
+        int tt[3], cc0[3], ttc[3], ee[3];
+        tile_extents<DIM>(m, tl, tl_i, tt, cc0, ttc, ee);
+        if (chk == 0)
+          load_brick<S>(bricks[bb], src, m, nt, cc0, ee);
+        const int first = chk * chunk;
+        for (int c = warp; c < chunk; c += nw)
+          {
+            const int lc = first + c;
+            const int lx = lc % TX, ly = (lc / TX) % TY, lz = lc / (TX * TY);
+            if (lc >= S::TC || lx >= ttc[0] || ly >= ttc[1] || lz >= ttc[2])
+              continue;
+            const long long cell = (cc0[0] + lx) + (long long)m.n[0] * ((cc0[1] + ly) + (long long)m.n[1] * (cc0[2] + lz));
+            const unsigned char *g = rec + cell * rec_bytes;
+            unsigned char       *d = recs[rb] + (long long)c * rec_bytes;
+            for (int q = lane; q < r16; q += 32)
+              cp_async16(d + 16 * q, g + 16 * q);
+          }
+      };
+
+      long long tile = blockIdx.x;
+      int       ch   = 0;
+      if (tile < tl.n_tiles)
+        issue(tile, 0, 0, 0);
+      cp_async_commit();
+      int rb = 0, bb = 0;
       int t[3], c0[3], tc[3], e[3];
-      tile_extents<DIM>(m, tl, blockIdx.x, t, c0, tc, e);
-      const int       nb    = e[0] * e[1] * e[2];
-      const int       nbmax = tl.E[0] * tl.E[1] * tl.E[2];
-      const int       tcmax = tl.T[0] * tl.T[1] * tl.T[2];
-      T              *zbuf  = brick + (long long)nt * nbmax;
-      T              *obuf  = zbuf + (long long)tcmax * nt * ND;
-      const long long N     = m.N;
-
-      for (int idx = threadIdx.x; idx < nt * nb; idx += blockDim.x)
+      while (tile < tl.n_tiles)
         {
-          const int i = idx / nb, r = idx % nb;
-          const int bx = r % e[0], by = (r / e[0]) % e[1], bz = r / (e[0] * e[1]);
-          const int gx = c0[0] * P + bx, gy = c0[1] * P + by, gz = c0[2] * P + bz;
-          T         v  = T(0);
-          if (!is_boundary_node(m, gx, gy, gz))
-            v = src[i * N + gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz)];
-          brick[i * nb + r] = v;
-        }
-      __syncthreads();
-
-      const int ncell = tc[0] * tc[1] * tc[2];
-      // B1: per (cell, mode): y = V^T x, z = (mu A + B)^{-1} y
-      for (int w = threadIdx.x; w < ncell * ND; w += blockDim.x)
-        {
-          const int lc = w / ND, mm = w % ND;
-          const int lx = lc % tc[0], ly = (lc / tc[0]) % tc[1], lz = lc / (tc[0] * tc[1]);
-          const long long cell = (c0[0] + lx) + (long long)m.n[0] * ((c0[1] + ly) + (long long)m.n[1] * (c0[2] + lz));
-          const TS *col = V + (cell * ND + mm) * ND;
-          T         y[NA], z[NA];
-#pragma unroll
-          for (int i = 0; i < NA; ++i)
-            y[i] = T(0);
-          const T *br = brick + lx * P + e[0] * (ly * P + e[1] * (lz * P));
-#pragma unroll
-          for (int a = 0; a < ND; ++a)
+          tile_extents<DIM>(m, tl, tile, t, c0, tc, e);
+          long long ntile = tile;
+          int       nchk  = ch + 1;
+          if (nchk >= nch)
             {
-              const int ax = a % P1, ay = (a / P1) % P1, az = a / (P1 * P1);
-              T         va;
-              if constexpr (sizeof(T) == 8)
-                va = T(col[a]);
-              else
-                va = load_s(col + a);
-              const T *bp = br + ax + e[0] * (ay + e[1] * az);
+              ntile = tile + gridDim.x;
+              nchk  = 0;
+            }
+          if (ntile < tl.n_tiles)
+            issue(ntile, nchk, rb ^ 1, nchk == 0 ? bb ^ 1 : bb);
+          cp_async_commit();
+          cp_async_wait<1>();
+          __syncthreads();
+
+          const T  *brick = bricks[bb];
+          const int first = ch * chunk;
+          // B1: per (cell, mode): y = V^T x, z = (mu A + B)^{-1} y
+          for (int w = threadIdx.x; w < chunk * ND; w += blockDim.x)
+            {
+              const int c = w / ND, mm = w - c * ND;
+              const int lc = first + c;
+              const int lx = lc % TX, ly = (lc / TX) % TY, lz = lc / (TX * TY);
+              if (lc >= S::TC || lx >= tc[0] || ly >= tc[1] || lz >= tc[2])
+                continue;
+              const unsigned char *r   = recs[rb] + (long long)c * rec_bytes;
+              const TS            *col = reinterpret_cast<const TS *>(r) + mm * ND;
+              const T              mu  = reinterpret_cast<const T *>(r + mu_off)[mm];
+              T                    y[NA], z[NA];
+#pragma unroll
+              for (int i = 0; i < NA; ++i)
+                y[i] = T(0);
+              const T *br = brick + lx * P + S::E0 * (ly * P + S::E1 * (lz * P));
+#pragma unroll
+              for (int a = 0; a < ND; ++a)
+                {
+                  T va;
+                  if constexpr (sizeof(T) == 8)
+                    va = T(col[a]);
+                  else
+                    va = load_s(col + a);
+                  const T *bp = br + S::offset(a);
+#pragma unroll
+                  for (int i = 0; i < NA; ++i)
+                    if (NT > 0 || i < nt)
+                      y[i] += va * bp[i * S::NB];
+                }
+              mode_solve<NT, T>(tm, mu, y, z, nt);
+              T *zb = zbuf + c * nt * ND + mm;
 #pragma unroll
               for (int i = 0; i < NA; ++i)
                 if (NT > 0 || i < nt)
-                  y[i] += va * bp[i * nb];
+                  zb[i * ND] = z[i];
             }
-          mode_solve<NT, T>(tm, mu[cell * ND + mm], y, z, nt);
-          T *zb = zbuf + (long long)lc * nt * ND + mm;
-#pragma unroll
-          for (int i = 0; i < NA; ++i)
-            if (NT > 0 || i < nt)
-              zb[i * ND] = z[i];
-        }
-      __syncthreads();
-      // B2: per (cell, node): out = V z
-      for (int w = threadIdx.x; w < ncell * ND; w += blockDim.x)
-        {
-          const int lc = w / ND, a = w % ND;
-          const int lx = lc % tc[0], ly = (lc / tc[0]) % tc[1], lz = lc / (tc[0] * tc[1]);
-          const long long cell = (c0[0] + lx) + (long long)m.n[0] * ((c0[1] + ly) + (long long)m.n[1] * (c0[2] + lz));
-          const TS *row = V + cell * ND * ND + a;
-          const T  *zb  = zbuf + (long long)lc * nt * ND;
-          T         o[NA];
-#pragma unroll
-          for (int i = 0; i < NA; ++i)
-            o[i] = T(0);
-#pragma unroll 4
-          for (int mm = 0; mm < ND; ++mm)
+          __syncthreads();
+          // B2: per (cell, dof): out = V z
+          for (int w = threadIdx.x; w < chunk * ND; w += blockDim.x)
             {
-              T vm;
-              if constexpr (sizeof(T) == 8)
-                vm = T(row[mm * ND]);
-              else
-                vm = load_s(row + mm * ND);
+              const int c = w / ND, a = w - c * ND;
+              const int lc = first + c;
+              const int lx = lc % TX, ly = (lc / TX) % TY, lz = lc / (TX * TY);
+              if (lc >= S::TC || lx >= tc[0] || ly >= tc[1] || lz >= tc[2])
+                continue;
+              const TS *vr = reinterpret_cast<const TS *>(recs[rb] + (long long)c * rec_bytes) + a;
+              const T  *zb = zbuf + c * nt * ND;
+              T         o[NA];
+#pragma unroll
+              for (int i = 0; i < NA; ++i)
+                o[i] = T(0);
+#pragma unroll 9
+              for (int mm = 0; mm < ND; ++mm)
+                {
+                  T vm;
+                  if constexpr (sizeof(T) == 8)
+                    vm = T(vr[mm * ND]);
+                  else
+                    vm = load_s(vr + mm * ND);
+#pragma unroll
+                  for (int i = 0; i < NA; ++i)
+                    if (NT > 0 || i < nt)
+                      o[i] += vm * zb[i * ND + mm];
+                }
 #pragma unroll
               for (int i = 0; i < NA; ++i)
                 if (NT > 0 || i < nt)
-                  o[i] += vm * zb[i * ND + mm];
+                  obuf[(i * S::TC + lc) * ND + a] = o[i];
             }
-          T *ob = obuf + (long long)lc * nt * ND + a;
-#pragma unroll
-          for (int i = 0; i < NA; ++i)
-            if (NT > 0 || i < nt)
-              ob[i * ND] = o[i];
-        }
-      __syncthreads();
-      // C: gather per brick node, weight 1/valence where complete
-      for (int idx = threadIdx.x; idx < nt * nb; idx += blockDim.x)
-        {
-          const int j = idx / nb, r = idx % nb;
-          const int b3[3] = {r % e[0], (r / e[0]) % e[1], r / (e[0] * e[1])};
-          int       lc0[3], nlc[3];
-#pragma unroll
-          for (int d = 0; d < 3; ++d)
+          __syncthreads();
+          if (ch == nch - 1)
             {
-              if (d >= DIM)
-                {
-                  lc0[d] = 0;
-                  nlc[d] = 1;
-                  continue;
-                }
-              const int q = b3[d] / P, rem = b3[d] % P;
-              if (rem == 0 && q > 0 && q < tc[d])
-                lc0[d] = q - 1, nlc[d] = 2;
-              else
-                lc0[d] = min(q, tc[d] - 1), nlc[d] = 1;
+              // C/D: coloured scatter into the output brick (this tile's input
+              // brick buffer, no longer read), then write with 1/valence
+              T *ob = bricks[bb];
+              scatter_cells<S, DIM, T>(obuf, ob, nt, tc);
+              write_brick<S, DIM, T, true>(ob, m, tl, tile, nt, c0, e, dst, shell, om);
+              __syncthreads();
+              bb ^= 1;
             }
-          T s = T(0);
-          for (int kz = 0; kz < nlc[2]; ++kz)
-            for (int ky = 0; ky < nlc[1]; ++ky)
-              for (int kx = 0; kx < nlc[0]; ++kx)
-                {
-                  const int cx = lc0[0] + kx, cy = lc0[1] + ky, cz = lc0[2] + kz;
-                  const int lc = cx + tc[0] * (cy + tc[1] * cz);
-                  const int ax = b3[0] - cx * P, ay = b3[1] - cy * P, az = DIM == 3 ? b3[2] - cz * P : 0;
-                  s += obuf[((long long)lc * nt + j) * ND + ax + P1 * (ay + P1 * az)];
-                }
-          bool interior = b3[0] > 0 && b3[0] < e[0] - 1 && b3[1] > 0 && b3[1] < e[1] - 1;
-          if (DIM == 3)
-            interior = interior && b3[2] > 0 && b3[2] < e[2] - 1;
-          if (interior)
-            {
-              const int       g[3] = {c0[0] * P + b3[0], c0[1] * P + b3[1], c0[2] * P + b3[2]};
-              const long long gi   = g[0] + (long long)m.nn[0] * (g[1] + (long long)m.nn[1] * g[2]);
-              dst[j * N + gi]      = s / T(valence_of(m, g));
-            }
-          else
-            shell[((long long)blockIdx.x * nt + j) * tl.tile_stride + shell_slot<DIM>(tl, e, b3[0], b3[1], b3[2])] = s;
+          rb ^= 1;
+          tile = ntile;
+          ch   = nchk;
         }
+      cp_async_wait<0>();
     }
 
     template <int DIM, typename T>
     __global__ void
-    vanka_fixup_kernel(const MeshView m, const Tiling tl, int nt, const T *__restrict__ shell, T *__restrict__ dst)
+    vanka_fixup_kernel(const MeshView m, const Tiling tl, int nt, const T *__restrict__ shell, T *__restrict__ dst,
+                       const OutMode<T> om)
     {
       const long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x;
       if (node >= m.N)
@@ -264,54 +276,108 @@ namespace stmg
         return;
       const T w = T(1) / T(valence_of(m, g));
       for (int j = 0; j < nt; ++j)
-        dst[j * m.N + node] = bd ? T(0) : shell_sum<DIM, T>(m, tl, shell, nt, j, g) * w;
+        {
+          const long long i = j * m.N + node;
+          if (bd)
+            om.write_constrained(dst, i);
+          else
+            om.write(dst, i, shell_sum<DIM, T>(m, tl, shell, nt, j, g) * w);
+        }
     }
+    // compile-time tile shapes of the Vanka apply (main and fallback)
+    template <int DIM, int P, bool BIG>
+    struct VkShape
+    {
+      static constexpr int TX = DIM == 2 ? (P <= 2 ? (BIG ? 8 : 2) : (P <= 4 ? (BIG ? 4 : 1) : (BIG ? 2 : 1)))
+                                         : (P == 1 ? (BIG ? 8 : 2) : (P == 2 ? (BIG ? 4 : 2) : (BIG ? 2 : 1)));
+      static constexpr int TY = TX;
+      static constexpr int TZ = DIM == 2 ? 1 : (P == 1 ? (BIG ? 4 : 2) : TX);
+    };
+
+    template <int DIM, int P, typename T, typename TS, int NT, bool BIG>
+    void
+    launch_apply3(const Vanka &vk, const T *src, T *dst, const OutMode<T> &om, cudaStream_t s)
+    {
+      using Sh = VkShape<DIM, P, BIG>;
+      const MeshView   &m    = vk.mesh->v;
+      const Tiling     &tl   = vk.tiling;
+      const std::size_t smem = vk.smem_bytes(vk.shape);
+      auto              kern = vanka_apply_kernel<DIM, P, T, TS, NT, Sh::TX, Sh::TY, Sh::TZ>;
+      const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, tl.n_tiles);
+      const TimeMats<T> &tm  = vk.tmats<T>();
+      kern<<<grid, 256, smem, s>>>(m, tl, tm, vk.V.ptr, vk.rec_bytes, vk.mu_off, vk.chunk, src, dst,
+                                   reinterpret_cast<T *>(vk.shell.ptr), om);
+      count_launch();
+      STMG_CUDA(cudaGetLastError());
+      if (tl.n_tiles > 1)
+        {
+          vanka_fixup_kernel<DIM, T>
+            <<<unsigned((m.N + 255) / 256), 256, 0, s>>>(m, tl, vk.nt, reinterpret_cast<T *>(vk.shell.ptr), dst, om);
+          count_launch();
+          STMG_CUDA(cudaGetLastError());
+        }
+    }
+
     template <int DIM, int P, typename T, typename TS, int NT>
     void
-    launch_apply3(const Vanka &vk, const T *src, T *dst, cudaStream_t s)
+    launch_apply_nt(const Vanka &vk, const T *src, T *dst, const OutMode<T> &om, cudaStream_t s)
     {
-      const MeshView &m    = vk.mesh->v;
-      const Tiling   &tl   = vk.tiling;
-      const std::size_t smem = vk.smem_bytes(tl);
-      auto kern = vanka_apply_kernel<DIM, P, T, TS, NT>;
-      STMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      const TimeMats<T> &tm = vk.tmats<T>();
-      kern<<<unsigned(tl.n_tiles), 256, smem, s>>>(m, tl, tm, reinterpret_cast<const TS *>(vk.V.ptr),
-                                                   reinterpret_cast<const T *>(vk.mu.ptr), src, dst,
-                                                   reinterpret_cast<T *>(vk.shell.ptr));
-      count_launch();
-      STMG_CUDA(cudaGetLastError());
-      vanka_fixup_kernel<DIM, T><<<unsigned((m.N + 255) / 256), 256, 0, s>>>(m, tl, vk.nt, reinterpret_cast<T *>(vk.shell.ptr), dst);
-      count_launch();
-      STMG_CUDA(cudaGetLastError());
+      if (vk.big)
+        launch_apply3<DIM, P, T, TS, NT, true>(vk, src, dst, om, s);
+      else
+        launch_apply3<DIM, P, T, TS, NT, false>(vk, src, dst, om, s);
     }
 
     template <int DIM, int P, typename T, typename TS>
     void
-    launch_apply2(const Vanka &vk, const T *src, T *dst, cudaStream_t s)
+    launch_apply2(const Vanka &vk, const T *src, T *dst, const OutMode<T> &om, cudaStream_t s)
     {
       switch (vk.nt)
         {
           case 2:
-            return launch_apply3<DIM, P, T, TS, 2>(vk, src, dst, s);
+            return launch_apply_nt<DIM, P, T, TS, 2>(vk, src, dst, om, s);
           case 3:
-            return launch_apply3<DIM, P, T, TS, 3>(vk, src, dst, s);
+            return launch_apply_nt<DIM, P, T, TS, 3>(vk, src, dst, om, s);
           case 4:
-            return launch_apply3<DIM, P, T, TS, 4>(vk, src, dst, s);
+            return launch_apply_nt<DIM, P, T, TS, 4>(vk, src, dst, om, s);
           default:
-            return launch_apply3<DIM, P, T, TS, 0>(vk, src, dst, s);
+            return launch_apply_nt<DIM, P, T, TS, 0>(vk, src, dst, om, s);
         }
     }
 
     template <int DIM, int P>
     void
-    launch_apply1(const Vanka &vk, const void *src, void *dst, cudaStream_t s)
+    launch_apply1(const Vanka &vk, const void *src, void *dst, double alpha, double beta, cudaStream_t s)
     {
+      const OutMode<double> o64{alpha, beta, nullptr};
+      const OutMode<float>  o32{float(alpha), float(beta), nullptr};
       if (vk.compute == STMG_F64)
-        return launch_apply2<DIM, P, double, double>(vk, static_cast<const double *>(src), static_cast<double *>(dst), s);
+        return launch_apply2<DIM, P, double, double>(vk, static_cast<const double *>(src), static_cast<double *>(dst),
+                                                     o64, s);
       if (vk.storage == STMG_BF16)
-        return launch_apply2<DIM, P, float, __nv_bfloat16>(vk, static_cast<const float *>(src), static_cast<float *>(dst), s);
-      return launch_apply2<DIM, P, float, float>(vk, static_cast<const float *>(src), static_cast<float *>(dst), s);
+        return launch_apply2<DIM, P, float, __nv_bfloat16>(vk, static_cast<const float *>(src),
+                                                           static_cast<float *>(dst), o32, s);
+      return launch_apply2<DIM, P, float, float>(vk, static_cast<const float *>(src), static_cast<float *>(dst), o32, s);
     }
   } // namespace vanka_detail
+
+  // compile-time Vanka tile shape for (dim, degree, main/fallback)
+  inline void
+  vanka_shape(int dim, int p, bool big, int *T3)
+  {
+#define STMG_VS(D, PP)                                                                                   \
+  if (dim == D && p == PP)                                                                               \
+    {                                                                                                    \
+      if (big)                                                                                           \
+        T3[0] = vanka_detail::VkShape<D, PP, true>::TX, T3[1] = vanka_detail::VkShape<D, PP, true>::TY,   \
+        T3[2] = vanka_detail::VkShape<D, PP, true>::TZ;                                                  \
+      else                                                                                               \
+        T3[0] = vanka_detail::VkShape<D, PP, false>::TX, T3[1] = vanka_detail::VkShape<D, PP, false>::TY, \
+        T3[2] = vanka_detail::VkShape<D, PP, false>::TZ;                                                 \
+      return;                                                                                            \
+    }
+    STMG_VS(2, 1) STMG_VS(2, 2) STMG_VS(2, 3) STMG_VS(2, 4) STMG_VS(2, 5) STMG_VS(3, 1) STMG_VS(3, 2) STMG_VS(3, 3)
+#undef STMG_VS
+    throw Error(STMG_ERR_UNSUPPORTED, "vanka: unsupported dim/degree");
+  }
 } // namespace stmg

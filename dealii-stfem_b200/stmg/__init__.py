@@ -82,6 +82,16 @@ def _stream(stream):
     return C.c_void_p(stream.cuda_stream)
 
 
+def time_weights(time_type, r, tau, n_steps, problem=HEAT):
+    """Alpha, Beta, rK, rM, rV of one slab (stmg_time_weights)."""
+    nt = (r + 1 if time_type == DG else r) * n_steps
+    A, B = np.zeros((nt, nt)), np.zeros((nt, nt))
+    rK, rM, rV = np.zeros(nt), np.zeros(nt), np.zeros(nt)
+    check(lib().stmg_time_weights(time_type, r, C.c_double(tau), n_steps, problem, _ptr(A), _ptr(B), _ptr(rK),
+                                  _ptr(rM), _ptr(rV)))
+    return A, B, rK, rM, rV
+
+
 class Mesh:
     """stmg_mesh_t: structured FE_Q(p) mesh level on the device."""
 
@@ -262,9 +272,12 @@ class Solver:
         check(lib().stmg_solver_run(self.h, n_slabs, its.ctypes.data_as(_ip), _stream(stream)))
         return its
 
-    def solution(self):
-        u = np.zeros(self.n_blocks * self.n_nodes)
-        v = np.zeros(self.n_blocks * self.n_nodes)
+    def solution(self, u=None, v=None, want_v=True):
+        """Last slab's blocks; u, v may be preallocated (e.g. pinned) arrays."""
+        if u is None:
+            u = np.zeros(self.n_blocks * self.n_nodes)
+        if v is None and want_v:
+            v = np.zeros(self.n_blocks * self.n_nodes)
         check(lib().stmg_solver_solution(self.h, _ptr(u), _ptr(v)))
         return u, v
 

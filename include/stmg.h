@@ -57,6 +57,17 @@ STMG_API int         stmg_version(void);
  * Diagnostic counter with no counterpart in the reference. */
 STMG_API int stmg_kernel_launches(long long *count);
 
+/* ---------------------------------------------------------- time algebra
+ * Time weights of one slab of n_steps steps of size tau for time degree r
+ * (time_type 1 = cGP, 2 = dG): get_fe_time_weights (fe_time.h:292-349) for
+ * the heat system (problem 1: Alpha, Beta and the right-hand-side columns
+ * rK, rM of tests/tp_01.cc:186-189) or the condensed wave system
+ * (problem 2: get_fe_time_weights_wave, fe_time.h:98-246, with rV). Host
+ * arrays: Alpha, Beta nt x nt, rK, rM, rV nt; nt = (r+1) n_steps (dG) or
+ * r n_steps (cGP). rV may be NULL for heat. */
+STMG_API int stmg_time_weights(int time_type, int r, double tau, int n_steps, int problem, double *Alpha,
+                               double *Beta, double *rK, double *rM, double *rV);
+
 /* ---------------------------------------------------------------- mesh
  * Structured hex mesh of n_cells[0] x n_cells[1] (x n_cells[2]) cells of
  * FE_Q(degree) on Gauss-Lobatto nodes with MappingQ1 and homogeneous
