@@ -254,4 +254,131 @@ namespace stmg
           }
     return s;
   }
+
+  // Fix-up of the nodes the tiles share, visited by family: nodes on
+  // interior x tile planes (owned by the tiles' x faces), then y planes
+  // (minus x-plane nodes), then z planes (minus x- and y-plane nodes), then
+  // the Dirichlet faces (each node once). Consecutive items walk a plane row,
+  // so the face-slot reads are coalesced.
+  struct FixupRanges
+  {
+    long long nx, ny, nz, nb;
+    long long total() const { return nx + ny + nz + nb; }
+  };
+
+  inline FixupRanges
+  fixup_ranges(const MeshView &m, const Tiling &tl)
+  {
+    const long long n0 = m.nn[0], n1 = m.nn[1], n2 = m.nn[2];
+    FixupRanges     r;
+    r.nx = (long long)(tl.ntiles[0] - 1) * n1 * n2;
+    r.ny = (long long)(tl.ntiles[1] - 1) * n0 * n2;
+    r.nz = m.dim == 3 ? (long long)(tl.ntiles[2] - 1) * n0 * n1 : 0;
+    r.nb = 2 * n1 * n2 + 2 * (n0 - 2) * n2 + (m.dim == 3 ? 2 * (n0 - 2) * (n1 - 2) : 0);
+    return r;
+  }
+
+  template <int DIM, typename T, bool WEIGHTED>
+  __global__ void
+  plane_fixup_kernel(const MeshView m, const Tiling tl, int nt, const T *__restrict__ shell, T *__restrict__ dst,
+                     const OutMode<T> om, const FixupRanges rg)
+  {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int n0 = m.nn[0], n1 = m.nn[1], n2 = m.nn[2];
+    const int sx = tl.T[0] * m.p, sy = tl.T[1] * m.p, sz = tl.T[2] * m.p;
+    int       g[3];
+    bool      boundary = false;
+    if (i < rg.nx)
+      {
+        const long long pl = (long long)n1 * n2;
+        g[0]               = int(1 + i / pl) * sx;
+        const long long r  = i % pl;
+        g[1]               = int(r % n1);
+        g[2]               = int(r / n1);
+      }
+    else if ((i -= rg.nx) < rg.ny)
+      {
+        const long long pl = (long long)n0 * n2;
+        g[1]               = int(1 + i / pl) * sy;
+        const long long r  = i % pl;
+        g[0]               = int(r % n0);
+        g[2]               = int(r / n0);
+        if (g[0] % sx == 0)
+          return; // on an x plane
+      }
+    else if ((i -= rg.ny) < rg.nz)
+      {
+        const long long pl = (long long)n0 * n1;
+        g[2]               = int(1 + i / pl) * sz;
+        const long long r  = i % pl;
+        g[0]               = int(r % n0);
+        g[1]               = int(r / n0);
+        if (g[0] % sx == 0 || g[1] % sy == 0)
+          return; // on an x or y plane
+      }
+    else if ((i -= rg.nz) < rg.nb)
+      {
+        boundary = true;
+        // x faces (all nodes), y faces (x interior), z faces (x, y interior)
+        const long long fx = 2ll * n1 * n2, fy = 2ll * (n0 - 2) * n2;
+        if (i < fx)
+          {
+            g[0] = (i < (long long)n1 * n2) ? 0 : n0 - 1;
+            const long long r = i % ((long long)n1 * n2);
+            g[1]              = int(r % n1);
+            g[2]              = int(r / n1);
+          }
+        else if ((i -= fx) < fy)
+          {
+            g[1] = (i < (long long)(n0 - 2) * n2) ? 0 : n1 - 1;
+            const long long r = i % ((long long)(n0 - 2) * n2);
+            g[0]              = 1 + int(r % (n0 - 2));
+            g[2]              = int(r / (n0 - 2));
+          }
+        else
+          {
+            i -= fy;
+            g[2] = (i < (long long)(n0 - 2) * (n1 - 2)) ? 0 : n2 - 1;
+            const long long r = i % ((long long)(n0 - 2) * (n1 - 2));
+            g[0]              = 1 + int(r % (n0 - 2));
+            g[1]              = 1 + int(r / (n0 - 2));
+          }
+      }
+    else
+      return;
+    const long long node = g[0] + (long long)n0 * (g[1] + (long long)n1 * g[2]);
+    if (boundary)
+      {
+        for (int j = 0; j < nt; ++j)
+          om.write_constrained(dst, j * m.N + node);
+        return;
+      }
+    if (is_boundary_node(m, g[0], g[1], g[2]))
+      return; // visited as a boundary item
+    T w = T(1);
+    if (WEIGHTED)
+      {
+        int v = 1;
+        for (int d = 0; d < DIM; ++d)
+          if (g[d] % m.p == 0)
+            v *= 2;
+        w = T(1) / T(v);
+      }
+    for (int j = 0; j < nt; ++j)
+      om.write(dst, j * m.N + node, shell_sum<DIM, T>(m, tl, shell, nt, j, g) * w);
+  }
+
+  template <int DIM, typename T, bool WEIGHTED>
+  inline void
+  launch_plane_fixup(const MeshView &m, const Tiling &tl, int nt, const T *shell, T *dst, const OutMode<T> &om,
+                     cudaStream_t s)
+  {
+    const FixupRanges rg = fixup_ranges(m, tl);
+    const long long   n  = rg.total();
+    if (n <= 0)
+      return;
+    plane_fixup_kernel<DIM, T, WEIGHTED><<<unsigned((n + 255) / 256), 256, 0, s>>>(m, tl, nt, shell, dst, om, rg);
+    count_launch();
+    STMG_CUDA(cudaGetLastError());
+  }
 } // namespace stmg

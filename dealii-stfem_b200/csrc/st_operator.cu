@@ -241,34 +241,6 @@ namespace stmg
       cp_async_wait<0>();
     }
 
-    // Fix-up: nodes on tile boundaries (and Dirichlet nodes) get the sum of
-    // their tiles' shell contributions in fixed order.
-    template <int DIM, typename T>
-    __global__ void
-    shell_fixup_kernel(const MeshView m, const Tiling tl, int nt, const T *__restrict__ shell, T *__restrict__ dst,
-                       const OutMode<T> om)
-    {
-      const long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-      if (node >= m.N)
-        return;
-      const int g[3] = {int(node % m.nn[0]), int((node / m.nn[0]) % m.nn[1]), int(node / ((long long)m.nn[0] * m.nn[1]))};
-      const bool bd = is_boundary_node(m, g[0], g[1], g[2]);
-      bool       on = false;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d)
-        on = on || (g[d] % (tl.T[d] * m.p) == 0);
-      if (!bd && !on)
-        return;
-      for (int j = 0; j < nt; ++j)
-        {
-          const long long i = j * m.N + node;
-          if (bd)
-            om.write_constrained(dst, i);
-          else
-            om.write(dst, i, shell_sum<DIM, T>(m, tl, shell, nt, j, g));
-        }
-    }
-
     // compile-time tile shape per (dim, degree, precision); the fallback
     // shape serves time dimensions whose bricks do not fit the main one
     template <int DIM, int P, typename T, bool BIG>
@@ -294,12 +266,7 @@ namespace stmg
       count_launch();
       STMG_CUDA(cudaGetLastError());
       if (tl.n_tiles > 1)
-        {
-          const unsigned nb = unsigned((m.N + 255) / 256);
-          shell_fixup_kernel<DIM, T><<<nb, 256, 0, s>>>(m, tl, tm.nt_out, shell, dst, om);
-          count_launch();
-          STMG_CUDA(cudaGetLastError());
-        }
+        launch_plane_fixup<DIM, T, false>(m, tl, tm.nt_out, shell, dst, om, s);
     }
 
     template <int DIM, int P, typename T>
@@ -413,6 +380,18 @@ namespace stmg
           shape_of<float>(mesh->v.dim, mesh->v.p, big, T3);
         if (smem_bytes(T3, nt_in_, nt_out_, elem) <= budget)
           {
+            // on small meshes the big tiles leave SMs idle: prefer the small
+            // shape when the big one yields fewer than two tiles per SM
+            if (big && make_tiling(mesh->v, T3).n_tiles < 2ll * sm_count())
+              {
+                int t3[3];
+                if (dtype == STMG_F64)
+                  shape_of<double>(mesh->v.dim, mesh->v.p, false, t3);
+                else
+                  shape_of<float>(mesh->v.dim, mesh->v.p, false, t3);
+                if (smem_bytes(t3, nt_in_, nt_out_, elem) <= budget)
+                  continue;
+              }
             big_out = big;
             for (int d = 0; d < 3; ++d)
               shape[d] = T3[d];

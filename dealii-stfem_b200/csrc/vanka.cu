@@ -496,7 +496,9 @@ namespace stmg
         for (int ch : {8, 4, 2, 1})
           {
             chunk = ch;
-            if (smem_bytes(shape) <= (b ? 112 : 200) * 1024)
+            // big tiles only where they give every SM two tiles or more
+            if (smem_bytes(shape) <= (b ? 112 : 200) * 1024 &&
+                (!b || make_tiling(mesh->v, shape).n_tiles >= 2ll * sm_count()))
               {
                 ok     = true;
                 big    = b;

@@ -90,16 +90,6 @@ namespace stmg
         }
     }
 
-    __device__ __forceinline__ int
-    valence_of(const MeshView &m, const int (&g)[3])
-    {
-      int v = 1;
-      for (int d = 0; d < m.dim; ++d)
-        if (g[d] % m.p == 0 && g[d] > 0 && g[d] < m.nn[d] - 1)
-          v *= 2;
-      return v;
-    }
-
     // Per cell the setup stores one record: V as [mode][dof] in the storage
     // type, padded to 16 bytes, then mu (nd values of the compute type),
     // padded to 16 bytes; rec_bytes = record stride. Records stream through
@@ -258,32 +248,6 @@ namespace stmg
       cp_async_wait<0>();
     }
 
-    template <int DIM, typename T>
-    __global__ void
-    vanka_fixup_kernel(const MeshView m, const Tiling tl, int nt, const T *__restrict__ shell, T *__restrict__ dst,
-                       const OutMode<T> om)
-    {
-      const long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-      if (node >= m.N)
-        return;
-      const int g[3] = {int(node % m.nn[0]), int((node / m.nn[0]) % m.nn[1]), int(node / ((long long)m.nn[0] * m.nn[1]))};
-      const bool bd = is_boundary_node(m, g[0], g[1], g[2]);
-      bool       on = false;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d)
-        on = on || (g[d] % (tl.T[d] * m.p) == 0);
-      if (!bd && !on)
-        return;
-      const T w = T(1) / T(valence_of(m, g));
-      for (int j = 0; j < nt; ++j)
-        {
-          const long long i = j * m.N + node;
-          if (bd)
-            om.write_constrained(dst, i);
-          else
-            om.write(dst, i, shell_sum<DIM, T>(m, tl, shell, nt, j, g) * w);
-        }
-    }
     // compile-time tile shapes of the Vanka apply (main and fallback)
     template <int DIM, int P, bool BIG>
     struct VkShape
@@ -310,12 +274,7 @@ namespace stmg
       count_launch();
       STMG_CUDA(cudaGetLastError());
       if (tl.n_tiles > 1)
-        {
-          vanka_fixup_kernel<DIM, T>
-            <<<unsigned((m.N + 255) / 256), 256, 0, s>>>(m, tl, vk.nt, reinterpret_cast<T *>(vk.shell.ptr), dst, om);
-          count_launch();
-          STMG_CUDA(cudaGetLastError());
-        }
+        launch_plane_fixup<DIM, T, true>(m, tl, vk.nt, reinterpret_cast<T *>(vk.shell.ptr), dst, om, s);
     }
 
     template <int DIM, int P, typename T, typename TS, int NT>
