@@ -13,6 +13,69 @@ namespace stmg
   {
     constexpr double PI = 3.14159265358979323846;
 
+    // ------------------------------------------------- dense tail helpers
+    using HMat = std::vector<double>; // row-major, host
+
+    // (n x k) (k x m)
+    HMat
+    hmul(const HMat &a, const HMat &b, long long n, long long k, long long m)
+    {
+      HMat c(std::size_t(n * m), 0.0);
+      for (long long i = 0; i < n; ++i)
+        for (long long p = 0; p < k; ++p)
+          {
+            const double aip = a[i * k + p];
+            if (aip == 0.0)
+              continue;
+            const double *bp = b.data() + p * m;
+            double       *ci = c.data() + i * m;
+            for (long long j = 0; j < m; ++j)
+              ci[j] += aip * bp[j];
+          }
+      return c;
+    }
+
+    // n_out x n_in matrix of a linear map on device FP64 vectors, applied to
+    // the columns of the identity
+    template <typename F>
+    HMat
+    dense_of(long long n_out, long long n_in, F &&apply, cudaStream_t s)
+    {
+      std::vector<double> h(std::size_t(n_in * n_in), 0.0);
+      for (long long j = 0; j < n_in; ++j)
+        h[j * n_in + j] = 1.0;
+      DevBuf<double> I(std::size_t(n_in * n_in)), Y(std::size_t(n_in * n_out));
+      I.upload(h);
+      for (long long j = 0; j < n_in; ++j)
+        apply(I.ptr + j * n_in, Y.ptr + j * n_out);
+      STMG_CUDA(cudaStreamSynchronize(s));
+      std::vector<double> y(std::size_t(n_in * n_out));
+      STMG_CUDA(cudaMemcpy(y.data(), Y.ptr, y.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      HMat out(std::size_t(n_out * n_in));
+      for (long long j = 0; j < n_in; ++j)
+        for (long long i = 0; i < n_out; ++i)
+          out[i * n_in + j] = y[j * n_out + i];
+      return out;
+    }
+
+    // y = C x, one warp per row, fixed reduction order
+    template <typename T>
+    __global__ void
+    dense_matvec_kernel(int n, const T *__restrict__ C, const T *__restrict__ x, T *__restrict__ y)
+    {
+      const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+      if (row >= n)
+        return;
+      T acc = T(0);
+      for (int j = lane; j < n; j += 32)
+        acc += C[(long long)row * n + j] * x[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0)
+        y[row] = acc;
+    }
+
     // ------------------------------------------------- right-hand side
     // VectorTools::create_right_hand_side with QGauss(p+1) for the
     // manufactured sources of tests/include/exact_solution.h:53-75 (heat)
@@ -240,18 +303,7 @@ namespace stmg
         lv.vanka  = std::make_unique<Vanka>(lv.mesh, lv.nt, lv.A.a.data(), lv.B.a.data(), dtype,
                                            dtype == STMG_F64 ? STMG_F64 : c.vanka_storage);
         if (l > 0)
-          {
-            const Level &co = levels[l - 1];
-            if (seq[l - 1] == tfe::NONE)
-              lv.to_coarser = std::make_unique<HTransfer>(lv.mesh, co.mesh, lv.nt, dtype);
-            else
-              {
-                const tfe::Mat P = seq[l - 1] == tfe::K ? tfe::projection(type, lv.r - 1, lv.r, lv.n_steps)
-                                                        : tfe::prolongation(type, lv.r, lv.n_steps);
-                STMG_REQUIRE(P.m == lv.nt && P.n == co.nt, STMG_ERR_SHAPE, "gmg: time transfer shape");
-                lv.to_coarser = std::make_unique<TTransfer>(lv.mesh, lv.nt, co.nt, P.a.data(), nullptr, dtype);
-              }
-          }
+          lv.to_coarser = make_transfer(l, dtype);
         const std::size_t bytes = std::size_t(lv.size()) * elem;
         lv.sol.alloc(bytes);
         lv.def.alloc(bytes);
@@ -265,6 +317,133 @@ namespace stmg
     for (int l = 1; l < L; ++l)
       levels[l].omega = dtype == STMG_F64 ? estimate_relaxation<double>(l, s) : estimate_relaxation<float>(l, s);
     STMG_CUDA(cudaDeviceSynchronize());
+    build_tail();
+  }
+
+  std::unique_ptr<Transfer>
+  GMG::make_transfer(int l, int dt) const
+  {
+    const Level &lv   = levels[l];
+    const Level &co   = levels[l - 1];
+    const auto   type = tfe::Type(cfg.time_type);
+    if (seq[l - 1] == tfe::NONE)
+      return std::make_unique<HTransfer>(lv.mesh, co.mesh, lv.nt, dt);
+    const tfe::Mat P = seq[l - 1] == tfe::K ? tfe::projection(type, lv.r - 1, lv.r, lv.n_steps)
+                                            : tfe::prolongation(type, lv.r, lv.n_steps);
+    STMG_REQUIRE(P.m == lv.nt && P.n == co.nt, STMG_ERR_SHAPE, "gmg: time transfer shape");
+    return std::make_unique<TTransfer>(lv.mesh, lv.nt, co.nt, P.a.data(), nullptr, dt);
+  }
+
+  // The levels 0..tail as one matrix. Per level, with W = omega P_vanka,
+  // M = I - W A and m sweeps, smoothing from zero is S = sum_{k<m} M^k W and
+  // post-smoothing maps x to M^m x + S d, so (Multigrid::level_v_step)
+  //   C_0 = S_0,  C_l = M_l^m (S_l + Pro_l C_{l-1} Res_l (I - A_l S_l)) + S_l.
+  // A, P_vanka, Pro and Res are read off the FP64 kernels column by column.
+  void
+  GMG::build_tail()
+  {
+    const char *e = std::getenv("STMG_DENSE_TAIL");
+    if (e && e[0] == '0')
+      return;
+    int t = -1;
+    for (int l = 0; l < int(levels.size()); ++l)
+      {
+        if (levels[l].size() > DENSE_TAIL_MAX)
+          break;
+        t = l;
+      }
+    if (t < 0)
+      return;
+    cudaStream_t s = nullptr;
+    HMat         C;
+    for (int l = 0; l <= t; ++l)
+      {
+        Level          &lv = levels[l];
+        const long long n  = lv.size();
+        StOperator      op(lv.mesh, lv.nt, lv.nt, lv.A.a.data(), lv.B.a.data(), STMG_F64);
+        Vanka           vk(lv.mesh, lv.nt, lv.A.a.data(), lv.B.a.data(), STMG_F64, STMG_F64);
+        const HMat      A = dense_of(n, n, [&](const double *x, double *y) { op.apply(false, x, y, false, s); }, s);
+        HMat            W = dense_of(n, n, [&](const double *x, double *y) { vk.apply(x, y, s); }, s);
+        for (double &w : W)
+          w *= lv.omega;
+        HMat M = hmul(W, A, n, n, n);
+        for (long long i = 0; i < n * n; ++i)
+          M[i] = (i / n == i % n ? 1.0 : 0.0) - M[i];
+        // binary powering: (M^a, S_a) with S_{a+b} = S_a + M^a S_b
+        const unsigned m = steps(l) * unsigned(cfg.smoothing_steps);
+        HMat           Mp = M, Sp = W, Mm, S;
+        bool           have = false;
+        for (unsigned bits = m;;)
+          {
+            if (bits & 1u)
+              {
+                if (!have)
+                  {
+                    Mm   = Mp;
+                    S    = Sp;
+                    have = true;
+                  }
+                else
+                  {
+                    HMat MS = hmul(Mm, Sp, n, n, n);
+                    for (long long i = 0; i < n * n; ++i)
+                      S[i] += MS[i];
+                    Mm = hmul(Mm, Mp, n, n, n);
+                  }
+              }
+            bits >>= 1;
+            if (!bits)
+              break;
+            HMat MS = hmul(Mp, Sp, n, n, n);
+            for (long long i = 0; i < n * n; ++i)
+              Sp[i] += MS[i];
+            Mp = hmul(Mp, Mp, n, n, n);
+          }
+        STMG_REQUIRE(have, STMG_ERR_ARG, "gmg: zero smoothing steps");
+        if (l == 0)
+          {
+            C = S;
+            continue;
+          }
+        const long long nc = levels[l - 1].size();
+        auto            tr = make_transfer(l, STMG_F64);
+        const HMat      Pro = dense_of(
+          n, nc,
+          [&](const double *x, double *y) {
+            fill<double>(n, 0.0, y, s);
+            tr->prolongate_add(x, y, s);
+          },
+          s);
+        const HMat Res = dense_of(
+          nc, n,
+          [&](const double *x, double *y) {
+            fill<double>(nc, 0.0, y, s);
+            tr->restrict_add(x, y, s);
+          },
+          s);
+        HMat IAS = hmul(A, S, n, n, n);
+        for (long long i = 0; i < n * n; ++i)
+          IAS[i] = (i / n == i % n ? 1.0 : 0.0) - IAS[i];
+        HMat X = hmul(Pro, hmul(C, hmul(Res, IAS, nc, n, n), nc, nc, n), n, nc, n);
+        for (long long i = 0; i < n * n; ++i)
+          X[i] += S[i];
+        C = hmul(Mm, X, n, n, n);
+        for (long long i = 0; i < n * n; ++i)
+          C[i] += S[i];
+      }
+    const long long n = levels[t].size();
+    if (dtype == STMG_F64)
+      {
+        tail_mat.alloc(std::size_t(n * n) * 8);
+        STMG_CUDA(cudaMemcpy(tail_mat.ptr, C.data(), std::size_t(n * n) * 8, cudaMemcpyHostToDevice));
+      }
+    else
+      {
+        std::vector<float> c32(C.begin(), C.end());
+        tail_mat.alloc(std::size_t(n * n) * 4);
+        STMG_CUDA(cudaMemcpy(tail_mat.ptr, c32.data(), std::size_t(n * n) * 4, cudaMemcpyHostToDevice));
+      }
+    tail = t;
   }
 
   std::vector<double>
@@ -317,6 +496,14 @@ namespace stmg
   GMG::vstep(int l, cudaStream_t s)
   {
     Level &lv = levels[l];
+    if (l == tail)
+      {
+        const long long n = lv.size();
+        dense_matvec_kernel<T><<<unsigned((n + 7) / 8), 256, 0, s>>>(int(n), as<T>(tail_mat), as<T>(lv.def), as<T>(lv.sol));
+        count_launch();
+        STMG_CUDA(cudaGetLastError());
+        return;
+      }
     if (l == 0)
       {
         // MGCoarseGridApplySmoother: smooth from zero (its first sweep

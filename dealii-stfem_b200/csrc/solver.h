@@ -58,6 +58,12 @@ namespace stmg
     std::vector<Level>  levels; // coarsest first
     int                 dtype;
     std::vector<tfe::MG> seq;
+    // Levels 0..tail (tail >= 0) run as one dense matrix C: with fixed
+    // relaxation weights and sweep counts the V-cycle from level `tail` down
+    // is the linear map sol = C def, composed once in FP64 from dense copies
+    // of the levels' operators, smoothers and transfers. -1: none.
+    int tail = -1;
+    static constexpr long long DENSE_TAIL_MAX = 256; // entries per level vector
 
   private:
     template <typename T>
@@ -71,6 +77,8 @@ namespace stmg
     template <typename T>
     double estimate_relaxation(int l, cudaStream_t s);
     unsigned steps(int l) const;
+    void     build_tail();
+    std::unique_ptr<Transfer> make_transfer(int l, int dt) const;
 
     SolverConfig    cfg;
     Blas           &blas;
@@ -78,6 +86,7 @@ namespace stmg
     cudaGraphExec_t graph     = nullptr;
     cudaStream_t    cap       = nullptr;
     long long       graph_nodes = 0;
+    DevBuf<unsigned char> tail_mat; // n x n row-major in the V-cycle's type
   };
 
   // FGMRES(restart) with CGS2 orthogonalisation on device vectors.
