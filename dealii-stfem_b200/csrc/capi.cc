@@ -245,6 +245,17 @@ extern "C"
   }
 
   int
+  stmg_op_vmult_box_noalloc(int dim, const int *n_cells, int degree, const double *lo, const double *hi,
+                            const void *coeff, int nt_out, int nt_in, const double *A, const double *B, int dtype,
+                            void *dst, const void *src, void *stream)
+  {
+    return guard([&] {
+      op_vmult_box_noalloc(dim, n_cells, degree, lo, hi, coeff, nt_out, nt_in, A, B, dtype, src, dst,
+                           static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
   stmg_op_Tvmult(stmg_op_t op, void *dst, const void *src, void *stream)
   {
     return guard([&] {

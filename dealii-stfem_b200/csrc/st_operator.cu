@@ -17,6 +17,8 @@
 // The result is deterministic (no atomics) and dst is written exactly once.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "st_operator.h"
 #include "tile_ops.cuh"
@@ -451,5 +453,171 @@ namespace stmg
         launch<float>(*this, transpose, static_cast<const float *>(src), static_cast<float *>(dst),
                       reinterpret_cast<float *>(shell.ptr), om, s);
       }
+  }
+} // namespace stmg
+
+// ---------------------------------------------------------------------------
+// Operator apply that allocates no device memory. The only scratch the
+// apply needs, the tiles' face slots, lives in one fixed array of this file's
+// device image, so every GPU that loads the library holds these bytes until
+// the process exits. Calls share the array: two calls whose kernels overlap
+// on the GPU (different streams, or different host threads on one device)
+// race on it. Nothing in it has to start at zero: every face slot the fix-up
+// reads is written by its tile earlier in the same call.
+namespace stmg
+{
+  constexpr std::size_t NOALLOC_SCRATCH_BYTES = std::size_t(16) << 20; // 16 MiB
+
+  static __device__ __align__(256) unsigned char noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+  namespace
+  {
+    constexpr int MAX_DEVICES = 64;
+    std::mutex    scratch_mutex;
+    void         *scratch_device_ptr[MAX_DEVICES] = {};
+
+    // Device address of noalloc_scratch on the current device, looked up on
+    // the first call per device (host code must not pass the array's name
+    // to a kernel: on the host it is only a stand-in for the symbol).
+    void *
+    scratch_address()
+    {
+      int dev = 0;
+      STMG_CUDA(cudaGetDevice(&dev));
+      STMG_REQUIRE(dev >= 0 && dev < MAX_DEVICES, STMG_ERR_CUDA, "op_vmult_box_noalloc: device ordinal out of range");
+      std::lock_guard<std::mutex> lock(scratch_mutex);
+      if (!scratch_device_ptr[dev])
+        {
+          void             *p = nullptr;
+          const cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);
+          if (e != cudaSuccess || !p)
+            throw Error(STMG_ERR_CUDA, std::string("op_vmult_box_noalloc: cudaGetSymbolAddress of the scratch array: ") +
+                                         cudaGetErrorString(e));
+          scratch_device_ptr[dev] = p;
+        }
+      return scratch_device_ptr[dev];
+    }
+
+    // the tiling StOperator::choose_tiling picks for these sizes
+    template <typename T>
+    Tiling
+    box_tiling(const MeshView &m, int nd, int nt_in, int nt_out, bool &big_out)
+    {
+      const std::size_t budget = 200 * 1024;
+      auto              smem   = [&](const int *sh) {
+        const std::size_t nb = std::size_t(sh[0] * m.p + 1) * (sh[1] * m.p + 1) * (m.dim == 3 ? sh[2] * m.p + 1 : 1);
+        const std::size_t tc = std::size_t(sh[0]) * sh[1] * (m.dim == 3 ? sh[2] : 1);
+        return sizeof(T) * (2 * std::size_t(std::max(nt_in, nt_out)) * nb + tc * nt_out * nd);
+      };
+      int big_sh[3], small_sh[3];
+      shape_of<T>(m.dim, m.p, true, big_sh);
+      shape_of<T>(m.dim, m.p, false, small_sh);
+      const bool big_fits = smem(big_sh) <= budget, small_fits = smem(small_sh) <= budget;
+      if (big_fits && !(make_tiling(m, big_sh).n_tiles < 2ll * sm_count() && small_fits))
+        {
+          big_out = true;
+          return make_tiling(m, big_sh);
+        }
+      STMG_REQUIRE(small_fits, STMG_ERR_UNSUPPORTED, "operator: time blocks do not fit in shared memory");
+      big_out = false;
+      return make_tiling(m, small_sh);
+    }
+
+    template <int DIM, int P, typename T, bool BIG>
+    void
+    launch_box(const MeshView &m, const Tiling &tl, const TimeMats<T> &tm, const Cart1D<T> &c1, const QTab<T> &qt,
+               const T *src, T *dst, T *shell, cudaStream_t s)
+    {
+      using Sh = OpShape<DIM, P, T, BIG>;
+      using S  = TileShape<DIM, P, Sh::TX, Sh::TY, Sh::TZ>;
+      const std::size_t smem = sizeof(T) * (2 * std::size_t(std::max(tm.nt_in, tm.nt_out)) * S::NB +
+                                            std::size_t(S::TC) * tm.nt_out * S::ND);
+      auto              kern = st_apply_kernel<DIM, P, T, true, Sh::TX, Sh::TY, Sh::TZ>;
+      const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, tl.n_tiles);
+      const OutMode<T>  om{T(1), T(0), nullptr};
+      kern<<<grid, 256, smem, s>>>(m, tl, tm, c1, qt, src, dst, shell, om);
+      count_launch();
+      STMG_CUDA(cudaGetLastError());
+      if (tl.n_tiles > 1)
+        launch_plane_fixup<DIM, T, false>(m, tl, tm.nt_out, shell, dst, om, s);
+    }
+
+    template <typename T>
+    void
+    box_apply(const MeshView &m, int nd, const double *A, const double *B, int nt_out, int nt_in, const T *src, T *dst,
+              cudaStream_t s)
+    {
+      bool         big = true;
+      const Tiling tl  = box_tiling<T>(m, nd, nt_in, nt_out, big);
+      const std::size_t need = tl.n_tiles > 1 ? std::size_t(tl.n_tiles) * nt_out * tl.tile_stride * sizeof(T) : 0;
+      if (need > NOALLOC_SCRATCH_BYTES)
+        throw Error(STMG_ERR_SHAPE, "op_vmult_box_noalloc: this mesh needs " + std::to_string(need) +
+                                      " bytes of tile scratch, more than the fixed " +
+                                      std::to_string(NOALLOC_SCRATCH_BYTES) + " bytes; use stmg_op_create instead");
+      T *shell = static_cast<T *>(scratch_address());
+      TimeMats<T> tm{};
+      tm.nt_out = nt_out;
+      tm.nt_in  = nt_in;
+      for (int k = 0; k < nt_out * nt_in; ++k)
+        {
+          tm.A[k] = T(A[k]);
+          tm.B[k] = T(B[k]);
+        }
+      const Cart1D<T> c1 = make_cart<T>(m);
+      const QTab<T>   qt = make_qtab<T>(m.p);
+#define STMG_BOX(D, PP)                                                                                  \
+  if (m.dim == D && m.p == PP)                                                                           \
+    return big ? launch_box<D, PP, T, true>(m, tl, tm, c1, qt, src, dst, shell, s)                       \
+               : launch_box<D, PP, T, false>(m, tl, tm, c1, qt, src, dst, shell, s);
+      STMG_BOX(2, 1) STMG_BOX(2, 2) STMG_BOX(2, 3) STMG_BOX(2, 4) STMG_BOX(2, 5)
+      STMG_BOX(3, 1) STMG_BOX(3, 2) STMG_BOX(3, 3) STMG_BOX(3, 4)
+#undef STMG_BOX
+      throw Error(STMG_ERR_UNSUPPORTED, "op_vmult_box_noalloc: unsupported dim/degree");
+    }
+  } // namespace
+
+  void
+  op_vmult_box_noalloc(int dim, const int *n_cells, int degree, const double *lo, const double *hi, const void *coeff,
+                       int nt_out, int nt_in, const double *A, const double *B, int dtype, const void *src, void *dst,
+                       cudaStream_t s)
+  {
+    STMG_REQUIRE(n_cells && lo && hi && A && B && src && dst, STMG_ERR_ARG, "op_vmult_box_noalloc: null argument");
+    STMG_REQUIRE(dim == 2 || dim == 3, STMG_ERR_ARG, "op_vmult_box_noalloc: dim must be 2 or 3");
+    STMG_REQUIRE(degree >= 1 && degree <= MAX_P && (dim == 2 || degree <= 4), STMG_ERR_UNSUPPORTED,
+                 "op_vmult_box_noalloc: degree must be 1..5 (3-D: 1..4)");
+    STMG_REQUIRE(nt_out >= 1 && nt_out <= MAX_NT && nt_in >= 1 && nt_in <= MAX_NT, STMG_ERR_ARG,
+                 "op_vmult_box_noalloc: time dimensions must be 1..16");
+    STMG_REQUIRE(dtype == STMG_F64 || dtype == STMG_F32, STMG_ERR_ARG, "op_vmult_box_noalloc: dtype must be F64 or F32");
+    // the view make_mesh builds for a uniform box (no vertex array needed)
+    MeshView m{};
+    m.dim    = dim;
+    m.p      = degree;
+    m.N      = 1;
+    m.ncells = 1;
+    for (int d = 0; d < 3; ++d)
+      {
+        STMG_REQUIRE(d >= dim || (n_cells[d] >= 1 && hi[d] > lo[d]), STMG_ERR_ARG,
+                     "op_vmult_box_noalloc: cell counts and box extents must be positive");
+        m.n[d]  = d < dim ? n_cells[d] : 1;
+        m.nn[d] = d < dim ? n_cells[d] * degree + 1 : 1;
+        m.h[d]  = d < dim ? (hi[d] - lo[d]) / n_cells[d] : 1.0;
+        if (d < dim)
+          {
+            m.N *= m.nn[d];
+            m.ncells *= m.n[d];
+          }
+      }
+    m.cartesian  = 1;
+    m.vert       = nullptr;
+    m.coeff_mode = coeff ? 1 : 0;
+    m.coeff64    = dtype == STMG_F64 ? static_cast<const double *>(coeff) : nullptr;
+    m.coeff32    = dtype == STMG_F32 ? static_cast<const float *>(coeff) : nullptr;
+    int nd = 1;
+    for (int d = 0; d < dim; ++d)
+      nd *= degree + 1;
+    if (dtype == STMG_F64)
+      box_apply<double>(m, nd, A, B, nt_out, nt_in, static_cast<const double *>(src), static_cast<double *>(dst), s);
+    else
+      box_apply<float>(m, nd, A, B, nt_out, nt_in, static_cast<const float *>(src), static_cast<float *>(dst), s);
   }
 } // namespace stmg

@@ -70,4 +70,11 @@ namespace stmg
     QTab<float>      qtab32;
     DevBuf<unsigned char> shell; // tile face slots (scratch, allocated at creation)
   };
+
+  // dst = (A (x) K + B (x) M) src on the uniform box [lo, hi] with n_cells
+  // cells, allocating no device memory (face slots in a fixed device array
+  // of st_operator.cu). coeff: per-cell coefficient in dtype, or null.
+  void op_vmult_box_noalloc(int dim, const int *n_cells, int degree, const double *lo, const double *hi,
+                            const void *coeff, int nt_out, int nt_in, const double *A, const double *B, int dtype,
+                            const void *src, void *dst, cudaStream_t s);
 } // namespace stmg

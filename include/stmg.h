@@ -93,6 +93,25 @@ STMG_API int stmg_op_destroy(stmg_op_t op);
 /* SystemMatrix::vmult (operators.h:94-122); with nt_in = 1 also
  * vmult(BlockVector&, const Vector&) (operators.h:182-187). */
 STMG_API int stmg_op_vmult(stmg_op_t op, void *dst, const void *src, void *stream);
+/* dst = (A (x) K + B (x) M) src on the uniform box [lo, hi] split into
+ * n_cells cells, computed like stmg_op_create + stmg_op_vmult on that mesh
+ * but with no handle and no device memory allocated by the call. It is for
+ * callers that cannot call cudaMalloc: a host application that owns the
+ * GPU's memory through its own pool or a fixed budget, or a solver loop that
+ * must not stall other streams on cudaMalloc's device-wide synchronisation.
+ * coeff: per-cell coefficient on the device in dtype (float for STMG_F32,
+ * double for STMG_F64), or NULL for 1. dst, src: device, nt x n_nodes.
+ * The tiles' face slots go to one fixed 16 MiB array in the library's device
+ * code, held on every GPU that loads the library until the process exits;
+ * a mesh that needs more returns STMG_ERR_SHAPE (in 3-D with Q2 and four
+ * time blocks, meshes up to about 48^3 cells fit). The first call on each
+ * device looks up that array's device address on the current device, so
+ * make it before any stream capture. All calls share the array: calls
+ * that run at the same time on one GPU race. No counterpart in the
+ * reference. */
+STMG_API int stmg_op_vmult_box_noalloc(int dim, const int *n_cells, int degree, const double *lo, const double *hi,
+                                       const void *coeff, int nt_out, int nt_in, const double *A, const double *B,
+                                       int dtype, void *dst, const void *src, void *stream);
 /* SystemMatrix::Tvmult (operators.h:124-152): A and B transposed. */
 STMG_API int stmg_op_Tvmult(stmg_op_t op, void *dst, const void *src, void *stream);
 /* SystemMatrix::vmult_add (operators.h:155-180): dst += op(src). */
