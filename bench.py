@@ -162,7 +162,7 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------- GPU arm
-def kernel_roofline(stmg, torch, w, kappa, hbm):
+def kernel_roofline(stmg, torch, w, kappa, hbm, only=None):
     """Finest-level FP32 operator and Vanka apply timed in isolation with CUDA
     events on the launching stream; algorithmic bytes per launch:
       operator: 2 n_t N 4 (read src, write dst) + cells 4 (coefficient)
@@ -175,10 +175,12 @@ def kernel_roofline(stmg, torch, w, kappa, hbm):
     y = torch.empty_like(x)
     s = torch.cuda.current_stream()
     out = {}
-    op = stmg.Operator(mesh, A, B, dtype=stmg.F32)
-    vk = stmg.Vanka(mesh, A, B, compute=stmg.F32, storage=stmg.F32)
+    op = stmg.Operator(mesh, A, B, dtype=stmg.F32) if only in (None, "st_apply") else None
+    vk = stmg.Vanka(mesh, A, B, compute=stmg.F32, storage=stmg.F32) if only in (None, "vanka_apply") else None
     for name, fn, nbytes in (("st_apply", lambda: op.vmult(y, x), 2 * nt * N * 4 + w["cells"] * 4),
                              ("vanka_apply", lambda: vk.vmult(y, x), w["cells"] * (27 * 27 + 27) * 4 + 2 * nt * N * 4)):
+        if only is not None and name != only:
+            continue
         for _ in range(3):
             fn()
         torch.cuda.synchronize()
@@ -320,7 +322,19 @@ def main():
     ap.add_argument("--refine", type=int, default=7, help="mesh 2^refine cells per direction (7: 128^3)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 V-cycle comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
+    ap.add_argument("--kernels-only", choices=["all", "st_apply", "vanka_apply"], default=None,
+                    help="only time the finest-level operator and/or Vanka apply in isolation (profiling)")
     args = ap.parse_args()
+    if args.kernels_only:
+        import torch
+        import stmg
+        w = workload(args.refine)
+        kappa, _ = inputs(w)
+        hbm, kind = peaks()
+        only = None if args.kernels_only == "all" else args.kernels_only
+        kr = kernel_roofline(stmg, torch, w, kappa, hbm, only)
+        print(json.dumps(dict(workload=w["name"], peak_gbs=hbm, peak_kind=kind, kernels=kr)), flush=True)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -12,40 +12,85 @@ namespace stmg
     constexpr int RED_BLOCKS  = 592; // 4 x 148 SMs
     constexpr int RED_THREADS = 256;
 
-    template <typename T>
-    __device__ __forceinline__ double
-    block_sum(double v, double *sh)
+    // Block sums of cnt per-thread values acc[0..cnt) into partial[blockIdx.x * cnt + i]:
+    // warp shuffles, then one thread per value over the warps (fixed order).
+    template <int MAXV>
+    __device__ __forceinline__ void
+    block_sums(double (&acc)[MAXV], int cnt, double *partial)
     {
-      for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_down_sync(0xffffffffu, v, o);
-      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-      if (lane == 0)
-        sh[warp] = v;
+      __shared__ double sh[RED_THREADS / 32][MAXV];
+      const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+      for (int i = 0; i < MAXV; ++i)
+        {
+          if (i >= cnt)
+            break;
+          double v = acc[i];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_down_sync(0xffffffffu, v, o);
+          if (lane == 0)
+            sh[warp][i] = v;
+        }
       __syncthreads();
-      double s = 0;
-      if (threadIdx.x == 0)
-        for (int w = 0; w < int(blockDim.x >> 5); ++w)
-          s += sh[w];
-      return s;
+      if (threadIdx.x < cnt)
+        {
+          double t = 0;
+          for (int w = 0; w < RED_THREADS / 32; ++w)
+            t += sh[w][threadIdx.x];
+          partial[blockIdx.x * cnt + threadIdx.x] = t;
+        }
     }
 
-    // partial[b * m + i] = sum over block b's slice of V_i . w
-    template <typename T>
-    __global__ void
-    multidot_partial(long long n, int m, const T *const *__restrict__ V, const T *__restrict__ w, double *partial)
+    // partial[b * m + i] = block b's share of V_i . w; w is read once
+    template <typename T, int MAXV>
+    __global__ void __launch_bounds__(RED_THREADS)
+    multidot_partial(long long n, int m, const __grid_constant__ VecPtrs V, const T *__restrict__ w, double *partial)
     {
-      __shared__ double sh[32];
-      for (int i = 0; i < m; ++i)
+      double acc[MAXV];
+#pragma unroll
+      for (int i = 0; i < MAXV; ++i)
+        acc[i] = 0;
+      for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
         {
-          const T *v = V[i];
-          double   s = 0;
-          for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-            s += double(v[k]) * double(w[k]);
-          const double t = block_sum<T>(s, sh);
-          if (threadIdx.x == 0)
-            partial[blockIdx.x * m + i] = t;
-          __syncthreads();
+          const double wk = double(w[k]);
+#pragma unroll
+          for (int i = 0; i < MAXV; ++i)
+            if (i < m)
+              acc[i] += double(__ldg(static_cast<const T *>(V.p[i]) + k)) * wk;
         }
+      block_sums<MAXV>(acc, m, partial);
+    }
+
+    // w -= sum_i c_i V_i; partial sums of w_new . w_new, then (if dots) of
+    // V_i . w_new; the second read of V_i[k] hits the thread's own L1 lines
+    template <typename T, int MAXV>
+    __global__ void __launch_bounds__(RED_THREADS)
+    orth_update_kernel(long long n, int m, const __grid_constant__ Coeffs c, const __grid_constant__ VecPtrs V,
+                       T *__restrict__ w, int dots, double *partial)
+    {
+      double acc[MAXV + 1];
+#pragma unroll
+      for (int i = 0; i <= MAXV; ++i)
+        acc[i] = 0;
+      for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        {
+          double s = double(w[k]);
+#pragma unroll
+          for (int i = 0; i < MAXV; ++i)
+            if (i < m)
+              s -= c.c[i] * double(__ldg(static_cast<const T *>(V.p[i]) + k));
+          const T st = T(s);
+          w[k]       = st;
+          const double sw = double(st);
+          acc[0] += sw * sw;
+          if (dots)
+#pragma unroll
+            for (int i = 0; i < MAXV; ++i)
+              if (i < m)
+                acc[i + 1] += double(__ldg(static_cast<const T *>(V.p[i]) + k)) * sw;
+        }
+      block_sums<MAXV + 1>(acc, dots ? m + 1 : 1, partial);
     }
 
     __global__ void
@@ -63,14 +108,15 @@ namespace stmg
     // w = alpha * w + sum_i c_i V_i   (c in kernel parameters)
     template <typename T>
     __global__ void
-    multi_axpy(long long n, int m, double alpha, const __grid_constant__ Coeffs c, const T *const *__restrict__ V,
+    multi_axpy(long long n, int m, double alpha, const __grid_constant__ Coeffs c, const __grid_constant__ VecPtrs V,
                T *__restrict__ w)
     {
       for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
         {
           double s = alpha == 0.0 ? 0.0 : alpha * double(w[k]);
+#pragma unroll 4
           for (int i = 0; i < m; ++i)
-            s += c.c[i] * double(V[i][k]);
+            s += c.c[i] * double(static_cast<const T *>(V.p[i])[k]);
           w[k] = T(s);
         }
     }
@@ -119,19 +165,28 @@ namespace stmg
 
   Blas::Blas()
   {
-    partial.alloc(std::size_t(RED_BLOCKS) * MAX_DOTS);
-    result.alloc(MAX_DOTS);
-    ptrs.alloc(MAX_DOTS * 2);
-    STMG_CUDA(cudaMallocHost(&host_result, MAX_DOTS * sizeof(double)));
-    STMG_CUDA(cudaMallocHost(&host_ptrs, MAX_DOTS * 2 * sizeof(void *)));
+    partial.alloc(std::size_t(RED_BLOCKS) * (MAX_DOTS + 1));
+    result.alloc(MAX_DOTS + 1);
+    STMG_CUDA(cudaMallocHost(&host_result, (MAX_DOTS + 1) * sizeof(double)));
   }
 
   Blas::~Blas()
   {
     if (host_result)
       cudaFreeHost(host_result);
-    if (host_ptrs)
-      cudaFreeHost(host_ptrs);
+  }
+
+  // reduce the block partials of m values and copy them to out (host)
+  void
+  Blas::fetch(int m, double *out, cudaStream_t s)
+  {
+    reduce_partials<<<1, 64, 0, s>>>(RED_BLOCKS, m, partial.ptr, result.ptr);
+    count_launch();
+    STMG_CUDA(cudaGetLastError());
+    STMG_CUDA(cudaMemcpyAsync(host_result, result.ptr, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    STMG_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < m; ++i)
+      out[i] = host_result[i];
   }
 
   template <typename T>
@@ -139,22 +194,18 @@ namespace stmg
   Blas::multidot(long long n, int m, const T *const *V, const T *w, double *out, cudaStream_t s)
   {
     STMG_REQUIRE(m >= 1 && m <= MAX_DOTS, STMG_ERR_ARG, "multidot: 1..32 vectors");
-    // vector pointers staged through pinned memory (ordered on the stream)
-    STMG_CUDA(cudaStreamSynchronize(s));
+    VecPtrs vp{};
     for (int i = 0; i < m; ++i)
-      host_ptrs[i] = const_cast<T *>(V[i]);
-    STMG_CUDA(cudaMemcpyAsync(ptrs.ptr, host_ptrs, m * sizeof(void *), cudaMemcpyHostToDevice, s));
-    multidot_partial<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, reinterpret_cast<const T *const *>(ptrs.ptr), w,
-                                                          partial.ptr);
+      vp.p[i] = V[i];
+    if (m <= 8)
+      multidot_partial<T, 8><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, vp, w, partial.ptr);
+    else if (m <= 16)
+      multidot_partial<T, 16><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, vp, w, partial.ptr);
+    else
+      multidot_partial<T, 32><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, vp, w, partial.ptr);
     count_launch();
     STMG_CUDA(cudaGetLastError());
-    reduce_partials<<<1, 32, 0, s>>>(RED_BLOCKS, m, partial.ptr, result.ptr);
-    count_launch();
-    STMG_CUDA(cudaGetLastError());
-    STMG_CUDA(cudaMemcpyAsync(host_result, result.ptr, m * sizeof(double), cudaMemcpyDeviceToHost, s));
-    STMG_CUDA(cudaStreamSynchronize(s));
-    for (int i = 0; i < m; ++i)
-      out[i] = host_result[i];
+    fetch(m, out, s);
   }
 
   template <typename T>
@@ -172,18 +223,45 @@ namespace stmg
   Blas::combine(long long n, double alpha, int m, const double *c, const T *const *V, T *w, cudaStream_t s)
   {
     STMG_REQUIRE(m >= 0 && m <= MAX_DOTS, STMG_ERR_ARG, "combine: 0..32 vectors");
-    Coeffs cc{};
+    Coeffs  cc{};
+    VecPtrs vp{};
     for (int i = 0; i < m; ++i)
-      cc.c[i] = c[i];
-    STMG_CUDA(cudaStreamSynchronize(s));
-    for (int i = 0; i < m; ++i)
-      host_ptrs[MAX_DOTS + i] = const_cast<T *>(V[i]);
-    void **dptr = reinterpret_cast<void **>(ptrs.ptr) + MAX_DOTS;
-    if (m > 0)
-      STMG_CUDA(cudaMemcpyAsync(dptr, host_ptrs + MAX_DOTS, m * sizeof(void *), cudaMemcpyHostToDevice, s));
-    multi_axpy<T><<<grid_for(n), 256, 0, s>>>(n, m, alpha, cc, reinterpret_cast<const T *const *>(dptr), w);
+      {
+        cc.c[i] = c[i];
+        vp.p[i] = V[i];
+      }
+    multi_axpy<T><<<grid_for(n), 256, 0, s>>>(n, m, alpha, cc, vp, w);
     count_launch();
     STMG_CUDA(cudaGetLastError());
+  }
+
+  template <typename T>
+  double
+  Blas::orth_update(long long n, int m, const double *c, const T *const *V, T *w, double *dots, cudaStream_t s)
+  {
+    STMG_REQUIRE(m >= 1 && m <= MAX_DOTS, STMG_ERR_ARG, "orth_update: 1..32 vectors");
+    Coeffs  cc{};
+    VecPtrs vp{};
+    for (int i = 0; i < m; ++i)
+      {
+        cc.c[i] = c[i];
+        vp.p[i] = V[i];
+      }
+    const int d = dots ? 1 : 0;
+    if (m <= 8)
+      orth_update_kernel<T, 8><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, cc, vp, w, d, partial.ptr);
+    else if (m <= 16)
+      orth_update_kernel<T, 16><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, cc, vp, w, d, partial.ptr);
+    else
+      orth_update_kernel<T, 32><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, cc, vp, w, d, partial.ptr);
+    count_launch();
+    STMG_CUDA(cudaGetLastError());
+    double out[MAX_DOTS + 1];
+    fetch(dots ? m + 1 : 1, out, s);
+    if (dots)
+      for (int i = 0; i < m; ++i)
+        dots[i] = out[i + 1];
+    return out[0];
   }
 
   template <typename Tout, typename Tin>
@@ -226,6 +304,7 @@ namespace stmg
   template void   Blas::multidot<T>(long long, int, const T *const *, const T *, double *, cudaStream_t);  \
   template double Blas::dot<T>(long long, const T *, const T *, cudaStream_t);                              \
   template void   Blas::combine<T>(long long, double, int, const double *, const T *const *, T *, cudaStream_t); \
+  template double Blas::orth_update<T>(long long, int, const double *, const T *const *, T *, double *, cudaStream_t); \
   template void   axpby<T>(long long, T, const T *, T, T *, cudaStream_t);                                  \
   template void   sub_from<T>(long long, const T *, T *, cudaStream_t);                                     \
   template void   fill<T>(long long, T, T *, cudaStream_t);

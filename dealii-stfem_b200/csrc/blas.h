@@ -12,8 +12,14 @@ namespace stmg
     double c[MAX_DOTS];
   };
 
+  // vector pointers of one call, passed by value to the kernels
+  struct VecPtrs
+  {
+    const void *p[MAX_DOTS];
+  };
+
   // Reductions with FP64 accumulation in a fixed order; owns its scratch
-  // (partial sums, pinned result and pointer staging), allocated once.
+  // (block partial sums and a pinned result), allocated once.
   class Blas
   {
   public:
@@ -30,12 +36,15 @@ namespace stmg
     // w = alpha w + sum_i c_i V_i
     template <typename T>
     void combine(long long n, double alpha, int m, const double *c, const T *const *V, T *w, cudaStream_t s);
+    // one Gram-Schmidt update in a single pass: w -= sum_i c_i V_i, then
+    // dots[i] = V_i . w (if dots) and returns w . w (synchronises)
+    template <typename T>
+    double orth_update(long long n, int m, const double *c, const T *const *V, T *w, double *dots, cudaStream_t s);
 
   private:
-    DevBuf<double>        partial, result;
-    DevBuf<void *>        ptrs;
-    double               *host_result = nullptr;
-    void                **host_ptrs   = nullptr;
+    void fetch(int m, double *out, cudaStream_t s);
+    DevBuf<double> partial, result;
+    double        *host_result = nullptr;
   };
 
   template <typename Tout, typename Tin>

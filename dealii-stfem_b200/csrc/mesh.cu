@@ -85,6 +85,7 @@ namespace stmg
                 v.cartesian = 0;
             }
         }
+    v.box = v.cartesian;
     if (coeff_mode == 2)
       v.cartesian = 0; // a coefficient varying inside cells needs quadrature
     m->vert_d.upload(m->vert_h);

@@ -14,48 +14,113 @@ namespace stmg
     constexpr double PI = 3.14159265358979323846;
 
     // ------------------------------------------------- dense tail helpers
-    using HMat = std::vector<double>; // row-major, host
-
-    // (n x k) (k x m)
-    HMat
-    hmul(const HMat &a, const HMat &b, long long n, long long k, long long m)
+    // Device FP64 matrices, column-major: M(i, j) = m[i + j * rows].
+    struct DMat
     {
-      HMat c(std::size_t(n * m), 0.0);
-      for (long long i = 0; i < n; ++i)
-        for (long long p = 0; p < k; ++p)
+      long long      rows = 0, cols = 0;
+      DevBuf<double> m;
+      DMat() = default;
+      DMat(long long r, long long c)
+        : rows(r)
+        , cols(c)
+        , m(std::size_t(r * c))
+      {}
+    };
+
+    // C = A B (+ C if acc), 32 x 32 tiles through shared memory
+    __global__ void
+    dgemm_kernel(long long n, long long k, long long m, const double *__restrict__ A, const double *__restrict__ B,
+                 double *__restrict__ C, int acc)
+    {
+      __shared__ double As[32][33], Bs[32][33];
+      const int       tx = threadIdx.x & 31, ty = threadIdx.x >> 5; // 32 x 8 threads
+      const long long i0 = blockIdx.x * 32ll, j0 = blockIdx.y * 32ll;
+      double          c[4] = {0, 0, 0, 0};
+      for (long long p0 = 0; p0 < k; p0 += 32)
+        {
+          for (int r = ty; r < 32; r += 8)
+            {
+              const long long i = i0 + tx, p = p0 + r; // A(i, p): column p, row i
+              As[r][tx]         = (i < n && p < k) ? A[i + p * n] : 0.0;
+              const long long pp = p0 + tx, j = j0 + r; // B(pp, j)
+              Bs[r][tx]          = (pp < k && j < m) ? B[pp + j * k] : 0.0;
+            }
+          __syncthreads();
+#pragma unroll 8
+          for (int q = 0; q < 32; ++q)
+            {
+              const double av = As[q][tx];
+#pragma unroll
+              for (int u = 0; u < 4; ++u)
+                c[u] += av * Bs[ty + 8 * u][q];
+            }
+          __syncthreads();
+        }
+      const long long i = i0 + tx;
+      if (i < n)
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
           {
-            const double aip = a[i * k + p];
-            if (aip == 0.0)
-              continue;
-            const double *bp = b.data() + p * m;
-            double       *ci = c.data() + i * m;
-            for (long long j = 0; j < m; ++j)
-              ci[j] += aip * bp[j];
+            const long long j = j0 + ty + 8 * u;
+            if (j < m)
+              C[i + j * n] = (acc ? C[i + j * n] : 0.0) + c[u];
           }
-      return c;
     }
 
-    // n_out x n_in matrix of a linear map on device FP64 vectors, applied to
-    // the columns of the identity
+    DMat
+    dmul(const DMat &A, const DMat &B, cudaStream_t s)
+    {
+      STMG_REQUIRE(A.cols == B.rows, STMG_ERR_SHAPE, "gmg: dense tail shapes");
+      DMat      C(A.rows, B.cols);
+      const dim3 grid(unsigned((A.rows + 31) / 32), unsigned((B.cols + 31) / 32));
+      dgemm_kernel<<<grid, 256, 0, s>>>(A.rows, A.cols, B.cols, A.m.ptr, B.m.ptr, C.m.ptr, 0);
+      STMG_CUDA(cudaGetLastError());
+      return C;
+    }
+
+    // y = a x + b y (+ c on the diagonal), elementwise over an n x n matrix
+    __global__ void
+    dcombine_kernel(long long n, double a, const double *__restrict__ x, double b, double *__restrict__ y, double diag)
+    {
+      const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+      if (i >= n * n)
+        return;
+      y[i] = a * x[i] + b * y[i] + (i / n == i % n ? diag : 0.0);
+    }
+
+    void
+    dcombine(double a, const DMat &x, double b, DMat &y, double diag, cudaStream_t s)
+    {
+      const long long n = y.rows;
+      dcombine_kernel<<<unsigned((n * n + 255) / 256), 256, 0, s>>>(n, a, x.m.ptr, b, y.m.ptr, diag);
+      STMG_CUDA(cudaGetLastError());
+    }
+
+    // matrix of a linear map on device FP64 vectors, applied to the columns
+    // of the identity (column j of the result = map(e_j))
     template <typename F>
-    HMat
+    DMat
     dense_of(long long n_out, long long n_in, F &&apply, cudaStream_t s)
     {
-      std::vector<double> h(std::size_t(n_in * n_in), 0.0);
+      DMat I(n_in, n_in), Y(n_out, n_in);
+      STMG_CUDA(cudaMemsetAsync(I.m.ptr, 0, sizeof(double) * n_in * n_in, s));
+      dcombine_kernel<<<unsigned((n_in * n_in + 255) / 256), 256, 0, s>>>(n_in, 0.0, I.m.ptr, 0.0, I.m.ptr, 1.0);
+      STMG_CUDA(cudaGetLastError());
       for (long long j = 0; j < n_in; ++j)
-        h[j * n_in + j] = 1.0;
-      DevBuf<double> I(std::size_t(n_in * n_in)), Y(std::size_t(n_in * n_out));
-      I.upload(h);
-      for (long long j = 0; j < n_in; ++j)
-        apply(I.ptr + j * n_in, Y.ptr + j * n_out);
-      STMG_CUDA(cudaStreamSynchronize(s));
-      std::vector<double> y(std::size_t(n_in * n_out));
-      STMG_CUDA(cudaMemcpy(y.data(), Y.ptr, y.size() * sizeof(double), cudaMemcpyDeviceToHost));
-      HMat out(std::size_t(n_out * n_in));
-      for (long long j = 0; j < n_in; ++j)
-        for (long long i = 0; i < n_out; ++i)
-          out[i * n_in + j] = y[j * n_out + i];
-      return out;
+        apply(I.m.ptr + j * n_in, Y.m.ptr + j * n_out);
+      return Y;
+    }
+
+    // row-major copy of a column-major matrix in the V-cycle's type
+    template <typename T>
+    __global__ void
+    to_rowmajor_kernel(long long n, const double *__restrict__ cm, T *__restrict__ rm)
+    {
+      const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+      if (e >= n * n)
+        return;
+      const long long r = e / n, c = e % n;
+      rm[e]             = T(cm[r + c * n]);
     }
 
     // y = C x, one warp per row, fixed reduction order
@@ -338,7 +403,8 @@ namespace stmg
   // M = I - W A and m sweeps, smoothing from zero is S = sum_{k<m} M^k W and
   // post-smoothing maps x to M^m x + S d, so (Multigrid::level_v_step)
   //   C_0 = S_0,  C_l = M_l^m (S_l + Pro_l C_{l-1} Res_l (I - A_l S_l)) + S_l.
-  // A, P_vanka, Pro and Res are read off the FP64 kernels column by column.
+  // A, P_vanka, Pro and Res are read off the FP64 kernels column by column;
+  // the products run as FP64 GEMMs on the device.
   void
   GMG::build_tail()
   {
@@ -355,94 +421,87 @@ namespace stmg
     if (t < 0)
       return;
     cudaStream_t s = nullptr;
-    HMat         C;
+    DMat         C;
     for (int l = 0; l <= t; ++l)
       {
         Level          &lv = levels[l];
         const long long n  = lv.size();
         StOperator      op(lv.mesh, lv.nt, lv.nt, lv.A.a.data(), lv.B.a.data(), STMG_F64);
         Vanka           vk(lv.mesh, lv.nt, lv.A.a.data(), lv.B.a.data(), STMG_F64, STMG_F64);
-        const HMat      A = dense_of(n, n, [&](const double *x, double *y) { op.apply(false, x, y, false, s); }, s);
-        HMat            W = dense_of(n, n, [&](const double *x, double *y) { vk.apply(x, y, s); }, s);
-        for (double &w : W)
-          w *= lv.omega;
-        HMat M = hmul(W, A, n, n, n);
-        for (long long i = 0; i < n * n; ++i)
-          M[i] = (i / n == i % n ? 1.0 : 0.0) - M[i];
+        const DMat      A = dense_of(n, n, [&](const double *x, double *y) { op.apply(false, x, y, false, s); }, s);
+        DMat            W = dense_of(n, n, [&](const double *x, double *y) { vk.apply(x, y, s); }, s);
+        dcombine(0.0, W, lv.omega, W, 0.0, s); // W = omega P_vanka
+        DMat M = dmul(W, A, s);
+        dcombine(0.0, M, -1.0, M, 1.0, s); // M = I - W A
         // binary powering: (M^a, S_a) with S_{a+b} = S_a + M^a S_b
         const unsigned m = steps(l) * unsigned(cfg.smoothing_steps);
-        HMat           Mp = M, Sp = W, Mm, S;
-        bool           have = false;
+        STMG_REQUIRE(m > 0, STMG_ERR_ARG, "gmg: zero smoothing steps");
+        DMat Mp = std::move(M), Sp = std::move(W), Mm, S;
+        bool have = false;
         for (unsigned bits = m;;)
           {
             if (bits & 1u)
               {
                 if (!have)
                   {
-                    Mm   = Mp;
-                    S    = Sp;
+                    Mm = DMat(n, n);
+                    S  = DMat(n, n);
+                    STMG_CUDA(cudaMemcpyAsync(Mm.m.ptr, Mp.m.ptr, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
+                    STMG_CUDA(cudaMemcpyAsync(S.m.ptr, Sp.m.ptr, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, s));
                     have = true;
                   }
                 else
                   {
-                    HMat MS = hmul(Mm, Sp, n, n, n);
-                    for (long long i = 0; i < n * n; ++i)
-                      S[i] += MS[i];
-                    Mm = hmul(Mm, Mp, n, n, n);
+                    const DMat MS = dmul(Mm, Sp, s);
+                    dcombine(1.0, MS, 1.0, S, 0.0, s);
+                    Mm = dmul(Mm, Mp, s);
                   }
               }
             bits >>= 1;
             if (!bits)
               break;
-            HMat MS = hmul(Mp, Sp, n, n, n);
-            for (long long i = 0; i < n * n; ++i)
-              Sp[i] += MS[i];
-            Mp = hmul(Mp, Mp, n, n, n);
+            const DMat MS = dmul(Mp, Sp, s);
+            dcombine(1.0, MS, 1.0, Sp, 0.0, s);
+            Mp = dmul(Mp, Mp, s);
           }
-        STMG_REQUIRE(have, STMG_ERR_ARG, "gmg: zero smoothing steps");
         if (l == 0)
           {
-            C = S;
+            C = std::move(S);
             continue;
           }
         const long long nc = levels[l - 1].size();
         auto            tr = make_transfer(l, STMG_F64);
-        const HMat      Pro = dense_of(
+        const DMat      Pro = dense_of(
           n, nc,
           [&](const double *x, double *y) {
             fill<double>(n, 0.0, y, s);
             tr->prolongate_add(x, y, s);
           },
           s);
-        const HMat Res = dense_of(
+        const DMat Res = dense_of(
           nc, n,
           [&](const double *x, double *y) {
             fill<double>(nc, 0.0, y, s);
             tr->restrict_add(x, y, s);
           },
           s);
-        HMat IAS = hmul(A, S, n, n, n);
-        for (long long i = 0; i < n * n; ++i)
-          IAS[i] = (i / n == i % n ? 1.0 : 0.0) - IAS[i];
-        HMat X = hmul(Pro, hmul(C, hmul(Res, IAS, nc, n, n), nc, nc, n), n, nc, n);
-        for (long long i = 0; i < n * n; ++i)
-          X[i] += S[i];
-        C = hmul(Mm, X, n, n, n);
-        for (long long i = 0; i < n * n; ++i)
-          C[i] += S[i];
+        DMat IAS = dmul(A, S, s);
+        dcombine(0.0, IAS, -1.0, IAS, 1.0, s); // I - A S
+        DMat X = dmul(Pro, dmul(C, dmul(Res, IAS, s), s), s);
+        dcombine(1.0, S, 1.0, X, 0.0, s);
+        C = dmul(Mm, X, s);
+        dcombine(1.0, S, 1.0, C, 0.0, s);
+        STMG_CUDA(cudaStreamSynchronize(s));
       }
     const long long n = levels[t].size();
+    tail_mat.alloc(std::size_t(n * n) * (dtype == STMG_F64 ? 8 : 4));
+    const unsigned nb = unsigned((n * n + 255) / 256);
     if (dtype == STMG_F64)
-      {
-        tail_mat.alloc(std::size_t(n * n) * 8);
-        STMG_CUDA(cudaMemcpy(tail_mat.ptr, C.data(), std::size_t(n * n) * 8, cudaMemcpyHostToDevice));
-      }
+      to_rowmajor_kernel<double><<<nb, 256, 0, s>>>(n, C.m.ptr, reinterpret_cast<double *>(tail_mat.ptr));
     else
-      {
-        std::vector<float> c32(C.begin(), C.end());
-        tail_mat.alloc(std::size_t(n * n) * 4);
-        STMG_CUDA(cudaMemcpy(tail_mat.ptr, c32.data(), std::size_t(n * n) * 4, cudaMemcpyHostToDevice));
-      }
+      to_rowmajor_kernel<float><<<nb, 256, 0, s>>>(n, C.m.ptr, reinterpret_cast<float *>(tail_mat.ptr));
+    STMG_CUDA(cudaGetLastError());
+    STMG_CUDA(cudaStreamSynchronize(s));
     tail = t;
   }
 
@@ -667,18 +726,15 @@ namespace stmg
           {
             P(Z[j].ptr, V[j].ptr);
             A(aux.ptr, Z[j].ptr);
-            // classical Gram-Schmidt, twice
-            std::vector<double> h(j + 1), h2(j + 1), neg(j + 1);
-            for (int pass = 0; pass < 2; ++pass)
-              {
-                blas.multidot<double>(n, j + 1, vp.data(), aux.ptr, (pass ? h2 : h).data(), s);
-                for (int i = 0; i <= j; ++i)
-                  neg[i] = -(pass ? h2 : h)[i];
-                blas.combine<double>(n, 1.0, j + 1, neg.data(), vp.data(), aux.ptr, s);
-              }
+            // classical Gram-Schmidt, twice, in three passes over the basis:
+            // h = V^T w; w -= V h with h2 = V^T w on the way; w -= V h2
+            std::vector<double> h(j + 1), h2(j + 1);
+            blas.multidot<double>(n, j + 1, vp.data(), aux.ptr, h.data(), s);
+            blas.orth_update<double>(n, j + 1, h.data(), vp.data(), aux.ptr, h2.data(), s);
+            const double hn2 = blas.orth_update<double>(n, j + 1, h2.data(), vp.data(), aux.ptr, nullptr, s);
             for (int i = 0; i <= j; ++i)
               H[i][j] = h[i] + h2[i];
-            const double hn = std::sqrt(blas.dot<double>(n, aux.ptr, aux.ptr, s));
+            const double hn = std::sqrt(hn2);
             H[j + 1][j]     = hn;
             if (hn != 0.0)
               axpby<double>(n, 1.0 / hn, aux.ptr, 0.0, V[j + 1].ptr, s);

@@ -63,7 +63,7 @@ namespace stmg
     // is the linear map sol = C def, composed once in FP64 from dense copies
     // of the levels' operators, smoothers and transfers. -1: none.
     int tail = -1;
-    static constexpr long long DENSE_TAIL_MAX = 256; // entries per level vector
+    static constexpr long long DENSE_TAIL_MAX = 4096; // entries per level vector
 
   private:
     template <typename T>

@@ -157,8 +157,72 @@ namespace stmg
           out[q] = b[q];
     }
 
-    template <int DIM, int P, typename T, bool CART, int TX, int TY, int TZ>
-    __global__ void __launch_bounds__(256, (sizeof(T) == 4 && CART) ? 2 : 1)
+    // K a + M b on an axis-parallel box cell (Jacobian diag(h)) with a
+    // coefficient per quadrature point: general_apply with the geometry
+    // folded into per-direction constants.
+    template <int DIM, int P, typename T>
+    __device__ __forceinline__ void
+    box_apply(const MeshView &m, const QTab<T> &qt, long long cell, T *a, T *b, T *out)
+    {
+      constexpr int P1 = P + 1;
+      constexpr int ND = Tens<P1, DIM>::ND;
+      sweep<P1, DIM, 0, false, false>(qt.S, a, a);
+      sweep<P1, DIM, 1, false, false>(qt.S, a, a);
+      sweep<P1, DIM, 0, false, false>(qt.S, b, b);
+      sweep<P1, DIM, 1, false, false>(qt.S, b, b);
+      if constexpr (DIM == 3)
+        {
+          sweep<P1, DIM, 2, false, false>(qt.S, a, a);
+          sweep<P1, DIM, 2, false, false>(qt.S, b, b);
+        }
+      T g0[ND], g1[ND], g2[DIM == 3 ? ND : 1];
+      sweep<P1, DIM, 0, false, false>(qt.Dq, a, g0);
+      sweep<P1, DIM, 1, false, false>(qt.Dq, a, g1);
+      if constexpr (DIM == 3)
+        sweep<P1, DIM, 2, false, false>(qt.Dq, a, g2);
+      T det = T(m.h[0]) * T(m.h[1]);
+      if constexpr (DIM == 3)
+        det *= T(m.h[2]);
+      const T ih0 = T(1) / (T(m.h[0]) * T(m.h[0])), ih1 = T(1) / (T(m.h[1]) * T(m.h[1]));
+      const T ih2 = DIM == 3 ? T(1) / (T(m.h[2]) * T(m.h[2])) : T(0);
+      const T *cq = m.coeff_mode == 2 ? (sizeof(T) == 8 ? reinterpret_cast<const T *>(m.coeff64)
+                                                         : reinterpret_cast<const T *>(m.coeff32)) +
+                                          cell * ND
+                                      : nullptr;
+      const T kcell = m.coeff_mode == 1 ? (sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell])) : T(1);
+#pragma unroll
+      for (int q = 0; q < ND; ++q)
+        {
+          const int qx = q % P1, qy = (q / P1) % P1, qz = q / (P1 * P1);
+          T         w  = qt.gw[qx] * qt.gw[qy];
+          if constexpr (DIM == 3)
+            w *= qt.gw[qz];
+          const T JxW = det * w;
+          const T k   = (cq ? cq[q] : kcell) * JxW;
+          g0[q] *= k * ih0;
+          g1[q] *= k * ih1;
+          if constexpr (DIM == 3)
+            g2[q] *= k * ih2;
+          b[q] *= JxW;
+        }
+      sweep<P1, DIM, 0, true, true>(qt.Dq, g0, b);
+      sweep<P1, DIM, 1, true, true>(qt.Dq, g1, b);
+      if constexpr (DIM == 3)
+        sweep<P1, DIM, 2, true, true>(qt.Dq, g2, b);
+      sweep<P1, DIM, 0, false, true>(qt.S, b, b);
+      if constexpr (DIM == 3)
+        {
+          sweep<P1, DIM, 1, false, true>(qt.S, b, b);
+          sweep<P1, DIM, 2, false, true>(qt.S, b, out);
+        }
+      else
+        sweep<P1, DIM, 1, false, true>(qt.S, b, out);
+    }
+
+    // MODE 1: cartesian cells, coefficient per cell (cart_apply); 2: box
+    // cells, coefficient per quadrature point (box_apply); 0: general
+    template <int DIM, int P, typename T, int MODE, int TX, int TY, int TZ>
+    __global__ void __launch_bounds__(256, (sizeof(T) == 4 && MODE == 1) ? 2 : 1)
     st_apply_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<T> tm,
                     const __grid_constant__ Cart1D<T> c1, const __grid_constant__ QTab<T> qt,
                     const T *__restrict__ src, T *__restrict__ dst, T *__restrict__ shell, const OutMode<T> om)
@@ -202,7 +266,7 @@ namespace stmg
               const int cx = c0[0] + lx, cy = c0[1] + ly, cz = c0[2] + lz;
               const long long cell = cx + (long long)m.n[0] * (cy + (long long)m.n[1] * cz);
               T kap = T(1);
-              if (CART && m.coeff_mode == 1)
+              if (MODE == 1 && m.coeff_mode == 1)
                 kap = sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell]);
               T a[ND], b[ND];
 #pragma unroll
@@ -223,8 +287,10 @@ namespace stmg
                       b[q] += be * br[S::offset(q)];
                 }
               T out[ND];
-              if constexpr (CART)
+              if constexpr (MODE == 1)
                 cart_apply<DIM, P>(c1, a, b, out);
+              else if constexpr (MODE == 2)
+                box_apply<DIM, P>(m, qt, cell, a, b, out);
               else
                 general_apply<DIM, P>(m, qt, cx, cy, cz, cell, a, b, out);
               T *cb = cellbuf + (j * S::TC + lc) * ND;
@@ -261,8 +327,9 @@ namespace stmg
     {
       using Sh = OpShape<DIM, P, T, BIG>;
       const MeshView &m    = op.mesh->v;
-      auto            kern = m.cartesian ? st_apply_kernel<DIM, P, T, true, Sh::TX, Sh::TY, Sh::TZ>
-                                         : st_apply_kernel<DIM, P, T, false, Sh::TX, Sh::TY, Sh::TZ>;
+      auto            kern = m.cartesian ? st_apply_kernel<DIM, P, T, 1, Sh::TX, Sh::TY, Sh::TZ>
+                             : (m.box ? st_apply_kernel<DIM, P, T, 2, Sh::TX, Sh::TY, Sh::TZ>
+                                      : st_apply_kernel<DIM, P, T, 0, Sh::TX, Sh::TY, Sh::TZ>);
       const unsigned  grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, tl.n_tiles);
       kern<<<grid, 256, smem, s>>>(m, tl, tm, op.cart<T>(), op.qtab<T>(), src, dst, shell, om);
       count_launch();
@@ -532,7 +599,7 @@ namespace stmg
       using S  = TileShape<DIM, P, Sh::TX, Sh::TY, Sh::TZ>;
       const std::size_t smem = sizeof(T) * (2 * std::size_t(std::max(tm.nt_in, tm.nt_out)) * S::NB +
                                             std::size_t(S::TC) * tm.nt_out * S::ND);
-      auto              kern = st_apply_kernel<DIM, P, T, true, Sh::TX, Sh::TY, Sh::TZ>;
+      auto              kern = st_apply_kernel<DIM, P, T, 1, Sh::TX, Sh::TY, Sh::TZ>;
       const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, tl.n_tiles);
       const OutMode<T>  om{T(1), T(0), nullptr};
       kern<<<grid, 256, smem, s>>>(m, tl, tm, c1, qt, src, dst, shell, om);

@@ -147,8 +147,9 @@ namespace stmg
     int       nn[3]; // nodes per direction
     long long N;     // nodes
     long long ncells;
-    int       cartesian;  // axis-aligned uniform cells
-    double    h[3];       // cell size (cartesian)
+    int       cartesian;  // axis-aligned uniform cells, coefficient constant per cell
+    int       box;        // axis-aligned uniform cells (any coefficient mode)
+    double    h[3];       // cell size (box / cartesian)
     const double *vert;   // vertex coordinates (general geometry), device
     int           coeff_mode; // 0 none, 1 per cell, 2 per quadrature point
     const double *coeff64;

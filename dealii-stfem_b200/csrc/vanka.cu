@@ -48,12 +48,45 @@ namespace stmg
 
     // --------------------------------------------------------------- setup
     // One CTA per cell: assemble K_c, M_c, factor, write V (as [m][a]) and mu.
+    // Record slot of cell cc in (tile, colour, cell) order: tiles of tl.T
+    // cells, colour = parity of the local cell coordinates, cells of one
+    // colour in lexicographic order of their half-coordinates.
+    __device__ __forceinline__ long long
+    record_slot(const Tiling &tl, int dim, const int (&cc)[3])
+    {
+      int       t[3], l[3];
+      long long tile = 0, stride = 1, tc = 1;
+      for (int d = 0; d < 3; ++d)
+        {
+          t[d] = cc[d] / tl.T[d];
+          l[d] = cc[d] - t[d] * tl.T[d];
+          tile += t[d] * stride;
+          stride *= tl.ntiles[d];
+          tc *= tl.T[d];
+        }
+      const int col = (l[0] & 1) | ((l[1] & 1) << 1) | ((l[2] & 1) << 2);
+      int       prefix = 0;
+      for (int c = 0; c < col; ++c)
+        {
+          int n = 1;
+          for (int d = 0; d < 3; ++d)
+            {
+              const int o = (c >> d) & 1;
+              n *= d < dim ? (tl.T[d] - o + 1) / 2 : (o ? 0 : 1);
+            }
+          prefix += n;
+        }
+      const int c0 = (tl.T[0] - (l[0] & 1) + 1) / 2, c1 = (tl.T[1] - (l[1] & 1) + 1) / 2;
+      const int idx = (l[0] >> 1) + c0 * ((l[1] >> 1) + c1 * (l[2] >> 1));
+      return tile * tc + prefix + idx;
+    }
+
     template <int DIM, int P, bool CART, typename TS>
     __global__ void
     vanka_setup_kernel(const MeshView m, const double *__restrict__ Kref, const double *__restrict__ Mref,
                        const double *__restrict__ elemK, const double *__restrict__ elemM,
                        unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int mu_double,
-                       int *__restrict__ status)
+                       int *__restrict__ status, const Tiling tl, int tiled)
     {
       constexpr int P1 = P + 1;
       constexpr int ND = Tens<P1, DIM>::ND;
@@ -65,6 +98,7 @@ namespace stmg
       const long long cell = blockIdx.x;
       const int cc[3] = {int(cell % m.n[0]), int((cell / m.n[0]) % m.n[1]), int(cell / ((long long)m.n[0] * m.n[1]))};
       const int tid = threadIdx.x, nth = blockDim.x;
+      const long long slot = tiled ? record_slot(tl, DIM, cc) : cell;
 
       // 1. patch matrices: global K, M restricted to the cell's dofs
       for (int e = tid; e < ND * ND; e += nth)
@@ -277,7 +311,7 @@ namespace stmg
                 s -= M[k][i] * Q[k][col];
               Q[i][col] = s / M[i][i];
             }
-          unsigned char *mr = rec + cell * rec_bytes + mu_off;
+          unsigned char *mr = rec + slot * rec_bytes + mu_off;
           if (mu_double)
             reinterpret_cast<double *>(mr)[col] = K[col][col];
           else
@@ -287,7 +321,7 @@ namespace stmg
       for (int e = tid; e < ND * ND; e += nth)
         {
           const int mm = e / ND, a = e % ND;
-          reinterpret_cast<TS *>(rec + cell * rec_bytes)[e] = to_storage<TS>(Q[a][mm]);
+          reinterpret_cast<TS *>(rec + slot * rec_bytes)[e] = to_storage<TS>(Q[a][mm]);
         }
     }
 
@@ -377,6 +411,12 @@ namespace stmg
     const int         p = mesh->v.p, dim = mesh->v.dim;
     const std::size_t nb = std::size_t(T3[0] * p + 1) * (T3[1] * p + 1) * (dim == 3 ? T3[2] * p + 1 : 1);
     const std::size_t tc = std::size_t(T3[0]) * T3[1] * (dim == 3 ? T3[2] : 1);
+    if (streamed)
+      {
+        const std::size_t ntp = nt == 3 ? 4 : nt;
+        return std::size_t(vanka_detail::VK_STAGES) * colour_cells * rec_bytes +
+               4 * (3 * nb * ntp + 8 * std::size_t(mesh->nd) * ntp);
+      }
     return 2ull * chunk * rec_bytes +
            elem * (2ull * nt * nb + std::size_t(chunk) * nt * mesh->nd + tc * nt * mesh->nd);
   }
@@ -434,7 +474,8 @@ namespace stmg
         STMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         (void)Vp;
         kern<<<unsigned(m.ncells), threads, smem>>>(m, Kref.ptr, Mref.ptr, eK.ptr, eM.ptr, vk.V.ptr, vk.rec_bytes,
-                                                    vk.mu_off, vk.compute == STMG_F64 ? 1 : 0, status.ptr);
+                                                    vk.mu_off, vk.compute == STMG_F64 ? 1 : 0, status.ptr, vk.tiling,
+                                                    vk.streamed ? 1 : 0);
         count_launch();
         STMG_CUDA(cudaGetLastError());
       };
@@ -479,15 +520,33 @@ namespace stmg
     auto              pad  = [](std::size_t b) { return (b + 15) / 16 * 16; };
     mu_off                 = int(pad(nd * nd * elem));
     rec_bytes              = int(pad(mu_off + nd * (compute == STMG_F64 ? 8 : 4)));
-    V.alloc(std::size_t(mesh->v.ncells) * rec_bytes);
-#define STMG_SETUP(D, PP)                                                                                \
-  if (dim == D && p == PP)                                                                               \
-    run_setup<D, PP>(*this);
-    STMG_SETUP(2, 1) STMG_SETUP(2, 2) STMG_SETUP(2, 3) STMG_SETUP(2, 4) STMG_SETUP(2, 5)
-    STMG_SETUP(3, 1) STMG_SETUP(3, 2) STMG_SETUP(3, 3)
-#undef STMG_SETUP
-    // compile-time tile shape and record chunk within a shared-memory budget
-    bool ok = false;
+    // compile-time tile shape: the streamed apply takes the main shape when
+    // two CTAs per SM fit, else the fallback; the other apply also sizes its
+    // record chunk within a shared-memory budget
+    streamed = compute == STMG_F32 && nt <= 4;
+    bool ok  = false;
+    for (bool b : {true, false})
+      {
+        if (!streamed || ok)
+          break;
+        vanka_shape(dim, p, b, shape);
+        tiling       = make_tiling(mesh->v, shape);
+        colour_cells = 1;
+        for (int c = 0; c < (1 << dim); ++c)
+          {
+            int n = 1;
+            for (int d = 0; d < dim; ++d)
+              n *= (tiling.T[d] - ((c >> d) & 1) + 1) / 2;
+            colour_cells = std::max(colour_cells, n);
+          }
+        if (smem_bytes(shape) <= (b ? 110 : 200) * 1024)
+          {
+            ok  = true;
+            big = b;
+          }
+      }
+    if (!ok)
+      streamed = false;
     for (bool b : {true, false})
       {
         if (ok)
@@ -508,6 +567,15 @@ namespace stmg
           }
       }
     STMG_REQUIRE(ok, STMG_ERR_UNSUPPORTED, "vanka: does not fit in shared memory");
+    const long long slots =
+      streamed ? tiling.n_tiles * (long long)tiling.T[0] * tiling.T[1] * tiling.T[2] : mesh->v.ncells;
+    V.alloc(std::size_t(slots) * rec_bytes);
+#define STMG_SETUP(D, PP)                                                                                \
+  if (dim == D && p == PP)                                                                               \
+    run_setup<D, PP>(*this);
+    STMG_SETUP(2, 1) STMG_SETUP(2, 2) STMG_SETUP(2, 3) STMG_SETUP(2, 4) STMG_SETUP(2, 5)
+    STMG_SETUP(3, 1) STMG_SETUP(3, 2) STMG_SETUP(3, 3)
+#undef STMG_SETUP
     shell.alloc(std::size_t(tiling.n_tiles) * nt * tiling.tile_stride * (compute == STMG_F64 ? 8 : 4));
   }
 

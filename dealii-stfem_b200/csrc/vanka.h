@@ -37,12 +37,26 @@ namespace stmg
     // 16 bytes, then the eigenvalues mu in the compute type, padded to 16 bytes
     DevBuf<unsigned char> V;
     int                   rec_bytes = 0, mu_off = 0, chunk = 8;
+    // streamed: FP32 compute with 1..4 time dofs; records are then stored in
+    // (tile, colour, cell) order, colour_cells records per colour at most
+    bool                  streamed = false;
+    int                   colour_cells = 1;
     bool                  big = true;                // compile-time tile shape in use
     int                   shape[3] = {1, 1, 1};
     DevBuf<unsigned char> shell; // tile face slots (scratch)
     TimeMats<double>      tm64;
     TimeMats<float>       tm32;
   };
+
+  // apply of one (dimension, degree), defined in vanka_apply_d<D>p<P>.cu
+  template <int D, int P>
+  void vanka_apply_dp(const Vanka &vk, const void *src, void *dst, double alpha, double beta, cudaStream_t s);
+#define STMG_VANKA_DP(D, P)                                                                              \
+  template <>                                                                                            \
+  void vanka_apply_dp<D, P>(const Vanka &vk, const void *src, void *dst, double alpha, double beta, cudaStream_t s);
+  STMG_VANKA_DP(2, 1) STMG_VANKA_DP(2, 2) STMG_VANKA_DP(2, 3) STMG_VANKA_DP(2, 4) STMG_VANKA_DP(2, 5)
+  STMG_VANKA_DP(3, 1) STMG_VANKA_DP(3, 2) STMG_VANKA_DP(3, 3)
+#undef STMG_VANKA_DP
 
   void vanka_apply_2d(const Vanka &vk, const void *src, void *dst, double alpha, double beta, cudaStream_t s);
   void vanka_apply_3d(const Vanka &vk, const void *src, void *dst, double alpha, double beta, cudaStream_t s);

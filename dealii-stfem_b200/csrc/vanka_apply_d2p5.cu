@@ -1,0 +1,12 @@
+// Vanka apply kernels for 2-D meshes of degree 5.
+#include "vanka_apply_impl.cuh"
+
+namespace stmg
+{
+  template <>
+  void
+  vanka_apply_dp<2, 5>(const Vanka &vk, const void *src, void *dst, double alpha, double beta, cudaStream_t s)
+  {
+    vanka_detail::launch_apply1<2, 5>(vk, src, dst, alpha, beta, s);
+  }
+} // namespace stmg

@@ -1,0 +1,12 @@
+// Vanka apply kernels for 3-D meshes of degree 3.
+#include "vanka_apply_impl.cuh"
+
+namespace stmg
+{
+  template <>
+  void
+  vanka_apply_dp<3, 3>(const Vanka &vk, const void *src, void *dst, double alpha, double beta, cudaStream_t s)
+  {
+    vanka_detail::launch_apply1<3, 3>(vk, src, dst, alpha, beta, s);
+  }
+} // namespace stmg

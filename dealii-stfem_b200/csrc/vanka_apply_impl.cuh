@@ -248,6 +248,391 @@ namespace stmg
       cp_async_wait<0>();
     }
 
+    // ------------------------------------------------ streamed FP32 apply
+    // (mu A + B) z = y for one mode in registers: Gaussian elimination with
+    // partial pivoting where the pivot row is brought up by compare-and-swap
+    // with static indices, so nothing is spilled to local memory.
+    template <int NT>
+    __device__ __forceinline__ void
+    mode_solve_reg(const TimeMats<float> &tm, float mu, const float (&y)[NT], float (&z)[NT])
+    {
+      float A[NT][NT + 1];
+#pragma unroll
+      for (int i = 0; i < NT; ++i)
+        {
+#pragma unroll
+          for (int j = 0; j < NT; ++j)
+            A[i][j] = fmaf(mu, tm.A[i * NT + j], tm.B[i * NT + j]);
+          A[i][NT] = y[i];
+        }
+#pragma unroll
+      for (int k = 0; k < NT; ++k)
+        {
+#pragma unroll
+          for (int i = k + 1; i < NT; ++i)
+            {
+              const bool sw = fabsf(A[i][k]) > fabsf(A[k][k]);
+#pragma unroll
+              for (int j = k; j <= NT; ++j)
+                {
+                  const float a = A[k][j], b = A[i][j];
+                  A[k][j]       = sw ? b : a;
+                  A[i][j]       = sw ? a : b;
+                }
+            }
+          const float d = __frcp_rn(A[k][k]);
+          A[k][k]       = d; // the back substitution multiplies by it
+#pragma unroll
+          for (int i = k + 1; i < NT; ++i)
+            {
+              const float f = A[i][k] * d;
+#pragma unroll
+              for (int j = k + 1; j <= NT; ++j)
+                A[i][j] -= f * A[k][j];
+            }
+        }
+#pragma unroll
+      for (int i = NT - 1; i >= 0; --i)
+        {
+          float s = A[i][NT];
+#pragma unroll
+          for (int j = i + 1; j < NT; ++j)
+            s -= A[i][j] * z[j];
+          z[i] = s * A[i][i];
+        }
+    }
+
+    // NT time values of one node, stored contiguously (NTP = padded count)
+    template <int NT>
+    struct TimeVec
+    {
+      static constexpr int NTP = NT == 3 ? 4 : NT;
+      __device__ __forceinline__ static void
+      load(const float *p, float (&v)[NT])
+      {
+        if constexpr (NTP == 4)
+          {
+            const float4 q = *reinterpret_cast<const float4 *>(p);
+            v[0]           = q.x;
+            v[1]           = q.y;
+            v[2]           = q.z;
+            if constexpr (NT == 4)
+              v[3] = q.w;
+          }
+        else if constexpr (NTP == 2)
+          {
+            const float2 q = *reinterpret_cast<const float2 *>(p);
+            v[0]           = q.x;
+            v[1]           = q.y;
+          }
+        else
+          v[0] = *p;
+      }
+      __device__ __forceinline__ static void
+      store(float *p, const float (&v)[NT])
+      {
+        if constexpr (NTP == 4)
+          *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], NT == 4 ? v[NT - 1] : 0.0f);
+        else if constexpr (NTP == 2)
+          *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
+        else
+          *p = v[0];
+      }
+    };
+
+    constexpr int VK_STAGES = 3; // record ring depth (colour phases in flight)
+
+    // Tile geometry in 32-bit integers (tile counts stay far below 2^31).
+    struct TileGeo
+    {
+      int c0[3], tc[3], e[3];
+    };
+
+    template <int DIM, int P>
+    __device__ __forceinline__ TileGeo
+    tile_geo(const MeshView &m, const Tiling &tl, int tile)
+    {
+      TileGeo   g;
+      const int t[3] = {tile % tl.ntiles[0], (tile / tl.ntiles[0]) % tl.ntiles[1], tile / (tl.ntiles[0] * tl.ntiles[1])};
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        {
+          g.c0[d] = t[d] * tl.T[d];
+          g.tc[d] = d < DIM ? min(tl.T[d], m.n[d] - g.c0[d]) : 1;
+          g.e[d]  = d < DIM ? g.tc[d] * P + 1 : 1;
+        }
+      return g;
+    }
+
+    // Streamed apply: the tile's cells are visited colour by colour (cells of
+    // one colour share no node), one warp per cell: modes over the lanes for
+    // y = V x and the n_t x n_t solves, dofs over the lanes for V^T z, which
+    // is added straight into the shared output brick (fixed order, no
+    // atomics). Records are stored in (tile, colour, cell) order, so each
+    // colour phase reads one contiguous block; blocks stream through a
+    // VK_STAGES ring of cp.async groups, one group per colour phase, the next
+    // tile's input brick riding in the group of its first phase. Bricks keep
+    // the time values of a node together (one vector load per node) and are
+    // moved by brick rows: each warp covers 32 / E0 rows per step.
+    template <int DIM, int P, typename TS, int NT, int TX, int TY, int TZ>
+    __global__ void __launch_bounds__(256, 2)
+    vanka_stream_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<float> tm,
+                        const unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int cpc,
+                        const float *__restrict__ src, float *__restrict__ dst, float *__restrict__ shell,
+                        const OutMode<float> om)
+    {
+      using S           = TileShape<DIM, P, TX, TY, TZ>;
+      using TV          = TimeVec<NT>;
+      constexpr int ND  = S::ND;
+      constexpr int NTP = TV::NTP;
+      constexpr int NC  = 1 << DIM;
+      constexpr int CPC = ((TX + 1) / 2) * ((TY + 1) / 2) * (DIM == 3 ? (TZ + 1) / 2 : 1);
+      constexpr int RPW = 32 / S::E0;                    // brick rows per warp step
+      constexpr int ROWS = NT * S::E1 * S::E2;          // rows of one brick (all time dofs)
+      constexpr int NW   = 8;                            // warps per CTA
+      static_assert(S::E0 <= 32, "brick rows wider than a warp");
+      extern __shared__ __align__(16) unsigned char vk_smem[];
+      __shared__ int col_n[NC], col_pre[NC], col_cell[NC][CPC];
+      const int       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const int       lrow = lane / S::E0, lx = lane - lrow * S::E0;
+      const long long stage_bytes = (long long)cpc * rec_bytes;
+      float          *bin0 = reinterpret_cast<float *>(vk_smem + VK_STAGES * stage_bytes);
+      float          *bout = bin0 + 2 * S::NB * NTP;
+      float          *zb   = bout + S::NB * NTP + warp * ND * NTP;
+      const long long tcr  = (long long)tl.T[0] * tl.T[1] * tl.T[2];
+      const int       my_tiles = int(blockIdx.x) < tl.n_tiles ? int((tl.n_tiles - 1 - blockIdx.x) / gridDim.x) + 1 : 0;
+      const int       phases   = my_tiles * NC;
+
+      // per colour: cell count, first record slot, local cell coordinates
+      if (threadIdx.x < NC)
+        {
+          const int col = threadIdx.x;
+          int       cnt[3], n = 1, pre = 0;
+          for (int c = 0; c <= col; ++c)
+            {
+              int nc = 1;
+#pragma unroll
+              for (int d = 0; d < 3; ++d)
+                {
+                  const int o = (c >> d) & 1;
+                  cnt[d]      = d < DIM ? (tl.T[d] - o + 1) / 2 : (o ? 0 : 1);
+                  nc *= cnt[d];
+                }
+              if (c < col)
+                pre += nc;
+              else
+                n = nc;
+            }
+          col_n[col]   = n;
+          col_pre[col] = pre;
+          for (int idx = 0; idx < n && idx < CPC; ++idx)
+            {
+              const int ix = idx % cnt[0], iy = (idx / cnt[0]) % cnt[1], iz = idx / (cnt[0] * cnt[1]);
+              const int cx = 2 * ix + (col & 1), cy = 2 * iy + ((col >> 1) & 1), cz = 2 * iz + ((col >> 2) & 1);
+              col_cell[col][idx] = cx | (cy << 8) | (cz << 16);
+            }
+        }
+      for (int idx = threadIdx.x; idx < S::NB * NTP; idx += blockDim.x)
+        bout[idx] = 0.0f;
+      __syncthreads();
+
+      auto issue = [&](int k) {
+        if (k < phases)
+          {
+            const int            tile = blockIdx.x + (k / NC) * gridDim.x;
+            const int            col  = k % NC;
+            const unsigned char *g    = rec + (tile * tcr + col_pre[col]) * rec_bytes;
+            unsigned char       *d    = vk_smem + (k % VK_STAGES) * stage_bytes;
+            const int            q16  = col_n[col] * (rec_bytes / 16);
+            for (int q = threadIdx.x; q < q16; q += blockDim.x)
+              cp_async16(d + 16 * q, g + 16 * q);
+            if (col == 0)
+              {
+                const TileGeo tg  = tile_geo<DIM, P>(m, tl, tile);
+                float        *bi  = bin0 + ((k / NC) & 1) * S::NB * NTP;
+                const int     gx  = tg.c0[0] * P + lx;
+                const bool    okx = lx < tg.e[0] && gx > 0 && gx < m.nn[0] - 1;
+                for (int rb = warp * RPW; rb < ROWS; rb += NW * RPW)
+                  {
+                    const int row = rb + lrow;
+                    if (lrow >= RPW || row >= ROWS)
+                      continue;
+                    const int  i = row / (S::E1 * S::E2), rem = row - i * (S::E1 * S::E2);
+                    const int  bz = rem / S::E1, by = rem - bz * S::E1;
+                    const int  gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
+                    bool       ok = okx && by < tg.e[1] && bz < tg.e[2] && gy > 0 && gy < m.nn[1] - 1;
+                    if (DIM == 3)
+                      ok = ok && gz > 0 && gz < m.nn[2] - 1;
+                    const float *gp = ok ? src + i * m.N + gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz) : src;
+                    cp_async_small<4>(bi + ((bz * S::E1 + by) * S::E0 + lx) * NTP + i, gp, ok);
+                  }
+              }
+          }
+        cp_async_commit();
+      };
+
+#pragma unroll
+      for (int k = 0; k < VK_STAGES - 1; ++k)
+        issue(k);
+
+      TileGeo tg{};
+      for (int k = 0; k < phases; ++k)
+        {
+          cp_async_wait<VK_STAGES - 2>();
+          __syncthreads(); // phase k's records visible; phase k-1 done (its stage and output adds)
+          issue(k + VK_STAGES - 1);
+
+          const int tile = blockIdx.x + (k / NC) * gridDim.x;
+          const int col  = k % NC;
+          if (col == 0)
+            tg = tile_geo<DIM, P>(m, tl, tile);
+          const int            n   = col_n[col];
+          const unsigned char *stg = vk_smem + (k % VK_STAGES) * stage_bytes;
+          const float         *bi  = bin0 + ((k / NC) & 1) * S::NB * NTP;
+          for (int idx = warp; idx < n; idx += NW)
+            {
+              const int cl = col_cell[col][idx];
+              const int cx = cl & 255, cy = (cl >> 8) & 255, cz = cl >> 16;
+              if (cx >= tg.tc[0] || cy >= tg.tc[1] || cz >= tg.tc[2])
+                continue;
+              const unsigned char *r    = stg + idx * rec_bytes;
+              const TS            *V    = reinterpret_cast<const TS *>(r);
+              const float         *mu   = reinterpret_cast<const float *>(r + mu_off);
+              const int            base = cx * P + S::E0 * (cy * P + S::E1 * (cz * P));
+              // y = V x per mode, then the mode's time solve
+              for (int mm = lane; mm < ND; mm += 32)
+                {
+                  float     y[NT];
+                  const TS *vr = V + mm * ND;
+                  if constexpr (NT == 4)
+                    {
+                      // packed FP32 pairs: two FFMA2 per node
+                      float2 y01 = make_float2(0.0f, 0.0f), y23 = y01;
+#pragma unroll
+                      for (int a = 0; a < ND; ++a)
+                        {
+                          const float  v  = load_s(vr + a);
+                          const float4 x  = *reinterpret_cast<const float4 *>(bi + (base + S::offset(a)) * NTP);
+                          const float2 vv = make_float2(v, v);
+                          y01             = __ffma2_rn(vv, make_float2(x.x, x.y), y01);
+                          y23             = __ffma2_rn(vv, make_float2(x.z, x.w), y23);
+                        }
+                      y[0] = y01.x;
+                      y[1] = y01.y;
+                      y[2] = y23.x;
+                      y[NT - 1] = y23.y;
+                    }
+                  else
+                    {
+#pragma unroll
+                      for (int i = 0; i < NT; ++i)
+                        y[i] = 0.0f;
+#pragma unroll
+                      for (int a = 0; a < ND; ++a)
+                        {
+                          const float v = load_s(vr + a);
+                          float       x[NT];
+                          TV::load(bi + (base + S::offset(a)) * NTP, x);
+#pragma unroll
+                          for (int i = 0; i < NT; ++i)
+                            y[i] = fmaf(v, x[i], y[i]);
+                        }
+                    }
+                  float z[NT];
+                  mode_solve_reg<NT>(tm, mu[mm], y, z);
+                  TV::store(zb + mm * NTP, z);
+                }
+              __syncwarp();
+              // out = V^T z per dof, added into the output brick
+              for (int a = lane; a < ND; a += 32)
+                {
+                  float o[NT];
+                  if constexpr (NT == 4)
+                    {
+                      float2 o01 = make_float2(0.0f, 0.0f), o23 = o01;
+#pragma unroll 9
+                      for (int mm = 0; mm < ND; ++mm)
+                        {
+                          const float  v  = load_s(V + mm * ND + a);
+                          const float4 z  = *reinterpret_cast<const float4 *>(zb + mm * NTP);
+                          const float2 vv = make_float2(v, v);
+                          o01             = __ffma2_rn(vv, make_float2(z.x, z.y), o01);
+                          o23             = __ffma2_rn(vv, make_float2(z.z, z.w), o23);
+                        }
+                      o[0] = o01.x;
+                      o[1] = o01.y;
+                      o[2] = o23.x;
+                      o[NT - 1] = o23.y;
+                    }
+                  else
+                    {
+#pragma unroll
+                      for (int i = 0; i < NT; ++i)
+                        o[i] = 0.0f;
+#pragma unroll 9
+                      for (int mm = 0; mm < ND; ++mm)
+                        {
+                          const float v = load_s(V + mm * ND + a);
+                          float       z[NT];
+                          TV::load(zb + mm * NTP, z);
+#pragma unroll
+                          for (int i = 0; i < NT; ++i)
+                            o[i] = fmaf(v, z[i], o[i]);
+                        }
+                    }
+                  float *ob = bout + (base + S::offset(a)) * NTP;
+                  float  cur[NT];
+                  TV::load(ob, cur);
+#pragma unroll
+                  for (int i = 0; i < NT; ++i)
+                    cur[i] += o[i];
+                  TV::store(ob, cur);
+                }
+              __syncwarp();
+            }
+          if (col == NC - 1)
+            {
+              __syncthreads();
+              // the tile's output: interior nodes -> dst (1/valence), shell
+              // nodes -> face slots (or constrained writes for one tile)
+              const int gx   = tg.c0[0] * P + lx;
+              const int vx   = (gx % P == 0) ? 2 : 1;
+              const bool inx = lx > 0 && lx < tg.e[0] - 1;
+              for (int rb = warp * RPW; rb < ROWS; rb += NW * RPW)
+                {
+                  const int row = rb + lrow;
+                  if (lrow >= RPW || row >= ROWS || lx >= tg.e[0])
+                    continue;
+                  const int j = row / (S::E1 * S::E2), rem = row - j * (S::E1 * S::E2);
+                  const int bz = rem / S::E1, by = rem - bz * S::E1;
+                  if (by >= tg.e[1] || bz >= tg.e[2])
+                    continue;
+                  const float sv   = bout[((bz * S::E1 + by) * S::E0 + lx) * NTP + j];
+                  bool        inte = inx && by > 0 && by < tg.e[1] - 1;
+                  if (DIM == 3)
+                    inte = inte && bz > 0 && bz < tg.e[2] - 1;
+                  const int       gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
+                  const long long gi = j * m.N + gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+                  if (inte)
+                    {
+                      int v = vx * ((gy % P == 0) ? 2 : 1);
+                      if (DIM == 3)
+                        v *= (gz % P == 0) ? 2 : 1;
+                      om.write(dst, gi, sv * (v == 1 ? 1.0f : (v == 2 ? 0.5f : (v == 4 ? 0.25f : 0.125f))));
+                    }
+                  else if (tl.n_tiles == 1)
+                    om.write_constrained(dst, gi);
+                  else
+                    shell[((long long)tile * NT + j) * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz)] = sv;
+                }
+              __syncthreads();
+              for (int idx = threadIdx.x; idx < S::NB * NTP; idx += blockDim.x)
+                bout[idx] = 0.0f;
+            }
+        }
+      cp_async_wait<0>();
+    }
+
     // compile-time tile shapes of the Vanka apply (main and fallback)
     template <int DIM, int P, bool BIG>
     struct VkShape
@@ -257,6 +642,53 @@ namespace stmg
       static constexpr int TY = TX;
       static constexpr int TZ = DIM == 2 ? 1 : (P == 1 ? (BIG ? 4 : 2) : TX);
     };
+
+    template <int DIM, int P, typename TS, int NT, bool BIG>
+    void
+    launch_stream(const Vanka &vk, const float *src, float *dst, const OutMode<float> &om, cudaStream_t s)
+    {
+      using Sh = VkShape<DIM, P, BIG>;
+      const MeshView   &m    = vk.mesh->v;
+      const Tiling     &tl   = vk.tiling;
+      const std::size_t smem = vk.smem_bytes(vk.shape);
+      auto              kern = vanka_stream_kernel<DIM, P, TS, NT, Sh::TX, Sh::TY, Sh::TZ>;
+      const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, tl.n_tiles);
+      kern<<<grid, 256, smem, s>>>(m, tl, vk.tmats<float>(), vk.V.ptr, vk.rec_bytes, vk.mu_off, vk.colour_cells,
+                                   src, dst, reinterpret_cast<float *>(vk.shell.ptr), om);
+      count_launch();
+      STMG_CUDA(cudaGetLastError());
+      if (tl.n_tiles > 1)
+        launch_plane_fixup<DIM, float, true>(m, tl, vk.nt, reinterpret_cast<float *>(vk.shell.ptr), dst, om, s);
+    }
+
+    template <int DIM, int P, typename TS, int NT>
+    void
+    launch_stream_nt(const Vanka &vk, const float *src, float *dst, const OutMode<float> &om, cudaStream_t s)
+    {
+      if (vk.big)
+        launch_stream<DIM, P, TS, NT, true>(vk, src, dst, om, s);
+      else
+        launch_stream<DIM, P, TS, NT, false>(vk, src, dst, om, s);
+    }
+
+    template <int DIM, int P, typename TS>
+    void
+    launch_stream_any(const Vanka &vk, const float *src, float *dst, const OutMode<float> &om, cudaStream_t s)
+    {
+      switch (vk.nt)
+        {
+          case 1:
+            return launch_stream_nt<DIM, P, TS, 1>(vk, src, dst, om, s);
+          case 2:
+            return launch_stream_nt<DIM, P, TS, 2>(vk, src, dst, om, s);
+          case 3:
+            return launch_stream_nt<DIM, P, TS, 3>(vk, src, dst, om, s);
+          case 4:
+            return launch_stream_nt<DIM, P, TS, 4>(vk, src, dst, om, s);
+          default:
+            throw Error(STMG_ERR_ARG, "vanka: streamed apply needs 1..4 time dofs");
+        }
+    }
 
     template <int DIM, int P, typename T, typename TS, int NT, bool BIG>
     void
@@ -313,6 +745,14 @@ namespace stmg
       if (vk.compute == STMG_F64)
         return launch_apply2<DIM, P, double, double>(vk, static_cast<const double *>(src), static_cast<double *>(dst),
                                                      o64, s);
+      if (vk.streamed)
+        {
+          if (vk.storage == STMG_BF16)
+            return launch_stream_any<DIM, P, __nv_bfloat16>(vk, static_cast<const float *>(src),
+                                                             static_cast<float *>(dst), o32, s);
+          return launch_stream_any<DIM, P, float>(vk, static_cast<const float *>(src), static_cast<float *>(dst), o32,
+                                                  s);
+        }
       if (vk.storage == STMG_BF16)
         return launch_apply2<DIM, P, float, __nv_bfloat16>(vk, static_cast<const float *>(src),
                                                            static_cast<float *>(dst), o32, s);
