@@ -63,7 +63,7 @@ namespace stmg
     }
 
     // w -= sum_i c_i V_i; partial sums of w_new . w_new, then (if dots) of
-    // V_i . w_new; the second read of V_i[k] hits the thread's own L1 lines
+    // V_i . w_new, with the V_i[k] kept in registers between the two uses
     template <typename T, int MAXV>
     __global__ void __launch_bounds__(RED_THREADS)
     orth_update_kernel(long long n, int m, const __grid_constant__ Coeffs c, const __grid_constant__ VecPtrs V,
@@ -75,20 +75,21 @@ namespace stmg
         acc[i] = 0;
       for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
         {
+          double v[MAXV];
           double s = double(w[k]);
 #pragma unroll
           for (int i = 0; i < MAXV; ++i)
-            if (i < m)
-              s -= c.c[i] * double(__ldg(static_cast<const T *>(V.p[i]) + k));
+            {
+              v[i] = i < m ? double(__ldg(static_cast<const T *>(V.p[i]) + k)) : 0.0;
+              s -= c.c[i] * v[i];
+            }
           const T st = T(s);
           w[k]       = st;
           const double sw = double(st);
           acc[0] += sw * sw;
-          if (dots)
 #pragma unroll
-            for (int i = 0; i < MAXV; ++i)
-              if (i < m)
-                acc[i + 1] += double(__ldg(static_cast<const T *>(V.p[i]) + k)) * sw;
+          for (int i = 0; i < MAXV; ++i)
+            acc[i + 1] += v[i] * sw;
         }
       block_sums<MAXV + 1>(acc, dots ? m + 1 : 1, partial);
     }

@@ -364,8 +364,47 @@ namespace stmg
             v *= 2;
         w = T(1) / T(v);
       }
-    for (int j = 0; j < nt; ++j)
-      om.write(dst, j * m.N + node, shell_sum<DIM, T>(m, tl, shell, nt, j, g) * w);
+    // the tiles holding the node: per direction the tile and the node's
+    // local index, a second tile where the node lies on a tile plane
+    int tt0[3], ll0[3], two[3], ee0[3], ee1[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      {
+        if (d >= DIM)
+          {
+            tt0[d] = 0, ll0[d] = 0, two[d] = 0, ee0[d] = ee1[d] = 1;
+            continue;
+          }
+        const int span = tl.T[d] * m.p;
+        two[d]         = g[d] % span == 0; // interior node on a tile plane (boundary nodes returned above)
+        tt0[d]         = two[d] ? g[d] / span - 1 : min(g[d] / span, tl.ntiles[d] - 1);
+        ll0[d]         = g[d] - tt0[d] * span;
+        ee0[d]         = min(tl.T[d], m.n[d] - tt0[d] * tl.T[d]) * m.p + 1;
+        ee1[d]         = two[d] ? min(tl.T[d], m.n[d] - (tt0[d] + 1) * tl.T[d]) * m.p + 1 : 1;
+      }
+    long long off[8];
+    bool      ok[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      {
+        const int ix = c & 1, iy = (c >> 1) & 1, iz = (c >> 2) & 1;
+        ok[c]        = !((ix && !two[0]) || (iy && !two[1]) || (iz && !two[2]));
+        const int e[3] = {ix ? ee1[0] : ee0[0], iy ? ee1[1] : ee0[1], iz ? ee1[2] : ee0[2]};
+        const long long tile = (tt0[0] + ix) + (long long)tl.ntiles[0] * ((tt0[1] + iy) + (long long)tl.ntiles[1] * (tt0[2] + iz));
+        off[c] = ok[c] ? tile * nt * tl.tile_stride +
+                           shell_slot<DIM>(tl, e, ix ? 0 : ll0[0], iy ? 0 : ll0[1], iz ? 0 : ll0[2])
+                       : 0;
+      }
+    long long gi = node;
+    for (int j = 0; j < nt; ++j, gi += m.N)
+      {
+        T s = T(0);
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (ok[c])
+            s += shell[off[c] + (long long)j * tl.tile_stride];
+        om.write(dst, gi, s * w);
+      }
   }
 
   template <int DIM, typename T, bool WEIGHTED>

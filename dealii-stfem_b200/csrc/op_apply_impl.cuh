@@ -1,0 +1,571 @@
+// Space-time operator kernels (see st_operator.cu for the method),
+// instantiated per (dimension, degree) by st_apply_d<D>p<P>.cu.
+#pragma once
+
+#include "async_copy.cuh"
+#include "kernels_common.cuh"
+#include "tile_ops.cuh"
+
+namespace stmg
+{
+  // everything one operator launch needs (host side)
+  template <typename T>
+  struct OpLaunch
+  {
+    MeshView     m;
+    Tiling       tl;
+    TimeMats<T>  tm;
+    Cart1D<T>    c1;
+    QTab<T>      qt;
+    const T     *src;
+    T           *dst;
+    T           *shell;
+    OutMode<T>   om;
+    bool         big;
+    cudaStream_t s;
+  };
+
+  // shared memory of the operator kernel for a tile shape: two input bricks
+  // (time values of a node contiguous, padded to ntp) and the per-cell results
+  inline int
+  op_ntp(int nt_in)
+  {
+    return nt_in <= 2 ? nt_in : (nt_in + 3) / 4 * 4;
+  }
+
+  inline std::size_t
+  op_smem_bytes(int dim, int p, const int *shape, int nt_in, int nt_out, std::size_t elem)
+  {
+    const std::size_t nb = std::size_t(shape[0] * p + 1) * (shape[1] * p + 1) * (dim == 3 ? shape[2] * p + 1 : 1);
+    const std::size_t tc = std::size_t(shape[0]) * shape[1] * (dim == 3 ? shape[2] : 1);
+    std::size_t       nd = 1;
+    for (int d = 0; d < dim; ++d)
+      nd *= p + 1;
+    return elem * (2 * std::size_t(op_ntp(nt_in)) * nb + tc * nt_out * nd);
+  }
+
+  template <int DIM, int P, typename T>
+  void op_launch_dp(const OpLaunch<T> &L);
+
+  namespace op_detail
+  {
+    template <int DIM, int P, typename T>
+    __device__ __forceinline__ void
+    cart_apply(const Cart1D<T> &c, T *a, T *b, T *out)
+    {
+      constexpr int P1 = P + 1;
+      constexpr int ND = Tens<P1, DIM>::ND;
+      if constexpr (DIM == 2)
+        {
+          // K a + M b = Kx (My a) + Mx (Ky a + My b)
+          T s[ND];
+          sweep<P1, 2, 1, false, false>(c.M[1], a, s);
+          sweep<P1, 2, 1, false, false>(c.K[1], a, a);
+          sweep<P1, 2, 1, true, false>(c.M[1], b, a);
+          sweep<P1, 2, 0, false, false>(c.K[0], s, out);
+          sweep<P1, 2, 0, true, false>(c.M[0], a, out);
+        }
+      else
+        {
+          // K a + M b = Kx (My Mz a) + Mx (Ky Mz a + My (Kz a + Mz b))
+          T s[ND], u[ND];
+          sweep<P1, 3, 2, false, false>(c.M[2], a, s);
+          sweep<P1, 3, 2, false, false>(c.K[2], a, a);
+          sweep<P1, 3, 2, true, false>(c.M[2], b, a);
+          sweep<P1, 3, 1, false, false>(c.M[1], s, u);
+          sweep<P1, 3, 1, false, false>(c.K[1], s, b);
+          sweep<P1, 3, 1, true, false>(c.M[1], a, b);
+          sweep<P1, 3, 0, false, false>(c.K[0], u, out);
+          sweep<P1, 3, 0, true, false>(c.M[0], b, out);
+        }
+    }
+
+    // K a + M b on a Q1-mapped cell with QGauss(p+1) and a coefficient per
+    // cell or per quadrature point.
+    template <int DIM, int P, typename T>
+    __device__ __forceinline__ void
+    general_apply(const MeshView &m, const QTab<T> &qt, int cx, int cy, int cz, long long cell, T *a, T *b, T *out)
+    {
+      constexpr int P1 = P + 1;
+      constexpr int ND = Tens<P1, DIM>::ND;
+      // values at the quadrature points
+      sweep<P1, DIM, 0, false, false>(qt.S, a, a);
+      sweep<P1, DIM, 1, false, false>(qt.S, a, a);
+      sweep<P1, DIM, 0, false, false>(qt.S, b, b);
+      sweep<P1, DIM, 1, false, false>(qt.S, b, b);
+      if constexpr (DIM == 3)
+        {
+          sweep<P1, DIM, 2, false, false>(qt.S, a, a);
+          sweep<P1, DIM, 2, false, false>(qt.S, b, b);
+        }
+      // reference gradients by collocation
+      T g0[ND], g1[ND], g2[DIM == 3 ? ND : 1];
+      sweep<P1, DIM, 0, false, false>(qt.Dq, a, g0);
+      sweep<P1, DIM, 1, false, false>(qt.Dq, a, g1);
+      if constexpr (DIM == 3)
+        sweep<P1, DIM, 2, false, false>(qt.Dq, a, g2);
+      T X[1 << DIM][DIM];
+      load_corners<DIM>(m, cx, cy, cz, X);
+      const T *cq    = nullptr;
+      T        kcell = T(1);
+      if constexpr (sizeof(T) == 8)
+        {
+          if (m.coeff_mode == 1)
+            kcell = T(m.coeff64[cell]);
+          else if (m.coeff_mode == 2)
+            cq = reinterpret_cast<const T *>(m.coeff64) + cell * ND;
+        }
+      else
+        {
+          if (m.coeff_mode == 1)
+            kcell = T(m.coeff32[cell]);
+          else if (m.coeff_mode == 2)
+            cq = reinterpret_cast<const T *>(m.coeff32) + cell * ND;
+        }
+#pragma unroll
+      for (int q = 0; q < ND; ++q)
+        {
+          const int qx = q % P1, qy = (q / P1) % P1, qz = q / (P1 * P1);
+          T         xi[3] = {qt.gx[qx], qt.gx[qy], DIM == 3 ? qt.gx[qz] : T(0)};
+          T         J[DIM][DIM], Ji[DIM][DIM];
+          q1_jacobian<DIM>(X, xi, J);
+          const T det = det_inv<DIM>(J, Ji);
+          T       w   = qt.gw[qx] * qt.gw[qy];
+          if constexpr (DIM == 3)
+            w *= qt.gw[qz];
+          const T JxW = fabs(det) * w;
+          const T k   = (cq ? cq[q] : kcell) * JxW;
+          // physical gradient Ji^T g, flux = k Ji (Ji^T g)
+          T gr[DIM] = {g0[q], g1[q]};
+          if constexpr (DIM == 3)
+            gr[2] = g2[q];
+          T ph[DIM];
+#pragma unroll
+          for (int i = 0; i < DIM; ++i)
+            {
+              T s = T(0);
+#pragma unroll
+              for (int d = 0; d < DIM; ++d)
+                s += Ji[d][i] * gr[d];
+              ph[i] = k * s;
+            }
+#pragma unroll
+          for (int d = 0; d < DIM; ++d)
+            {
+              T s = T(0);
+#pragma unroll
+              for (int i = 0; i < DIM; ++i)
+                s += Ji[d][i] * ph[i];
+              gr[d] = s;
+            }
+          g0[q] = gr[0];
+          g1[q] = gr[1];
+          if constexpr (DIM == 3)
+            g2[q] = gr[2];
+          b[q] *= JxW;
+        }
+      // integrate: collocation derivatives transposed, then S^T
+      sweep<P1, DIM, 0, true, true>(qt.Dq, g0, b);
+      sweep<P1, DIM, 1, true, true>(qt.Dq, g1, b);
+      if constexpr (DIM == 3)
+        sweep<P1, DIM, 2, true, true>(qt.Dq, g2, b);
+      sweep<P1, DIM, 0, false, true>(qt.S, b, b);
+      sweep<P1, DIM, 1, false, true>(qt.S, b, b);
+      if constexpr (DIM == 3)
+        sweep<P1, DIM, 2, false, true>(qt.S, b, out);
+      else
+#pragma unroll
+        for (int q = 0; q < ND; ++q)
+          out[q] = b[q];
+    }
+
+    // K a + M b on an axis-parallel box cell (Jacobian diag(h)) with a
+    // coefficient per quadrature point: general_apply with the geometry
+    // folded into per-direction constants.
+    template <int DIM, int P, typename T>
+    __device__ __forceinline__ void
+    box_apply(const MeshView &m, const QTab<T> &qt, long long cell, T *a, T *b, T *out)
+    {
+      constexpr int P1 = P + 1;
+      constexpr int ND = Tens<P1, DIM>::ND;
+      sweep<P1, DIM, 0, false, false>(qt.S, a, a);
+      sweep<P1, DIM, 1, false, false>(qt.S, a, a);
+      sweep<P1, DIM, 0, false, false>(qt.S, b, b);
+      sweep<P1, DIM, 1, false, false>(qt.S, b, b);
+      if constexpr (DIM == 3)
+        {
+          sweep<P1, DIM, 2, false, false>(qt.S, a, a);
+          sweep<P1, DIM, 2, false, false>(qt.S, b, b);
+        }
+      T g0[ND], g1[ND], g2[DIM == 3 ? ND : 1];
+      sweep<P1, DIM, 0, false, false>(qt.Dq, a, g0);
+      sweep<P1, DIM, 1, false, false>(qt.Dq, a, g1);
+      if constexpr (DIM == 3)
+        sweep<P1, DIM, 2, false, false>(qt.Dq, a, g2);
+      T det = T(m.h[0]) * T(m.h[1]);
+      if constexpr (DIM == 3)
+        det *= T(m.h[2]);
+      const T ih0 = T(1) / (T(m.h[0]) * T(m.h[0])), ih1 = T(1) / (T(m.h[1]) * T(m.h[1]));
+      const T ih2 = DIM == 3 ? T(1) / (T(m.h[2]) * T(m.h[2])) : T(0);
+      const T *cq = m.coeff_mode == 2 ? (sizeof(T) == 8 ? reinterpret_cast<const T *>(m.coeff64)
+                                                         : reinterpret_cast<const T *>(m.coeff32)) +
+                                          cell * ND
+                                      : nullptr;
+      const T kcell = m.coeff_mode == 1 ? (sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell])) : T(1);
+#pragma unroll
+      for (int q = 0; q < ND; ++q)
+        {
+          const int qx = q % P1, qy = (q / P1) % P1, qz = q / (P1 * P1);
+          T         w  = qt.gw[qx] * qt.gw[qy];
+          if constexpr (DIM == 3)
+            w *= qt.gw[qz];
+          const T JxW = det * w;
+          const T k   = (cq ? cq[q] : kcell) * JxW;
+          g0[q] *= k * ih0;
+          g1[q] *= k * ih1;
+          if constexpr (DIM == 3)
+            g2[q] *= k * ih2;
+          b[q] *= JxW;
+        }
+      sweep<P1, DIM, 0, true, true>(qt.Dq, g0, b);
+      sweep<P1, DIM, 1, true, true>(qt.Dq, g1, b);
+      if constexpr (DIM == 3)
+        sweep<P1, DIM, 2, true, true>(qt.Dq, g2, b);
+      sweep<P1, DIM, 0, false, true>(qt.S, b, b);
+      if constexpr (DIM == 3)
+        {
+          sweep<P1, DIM, 1, false, true>(qt.S, b, b);
+          sweep<P1, DIM, 2, false, true>(qt.S, b, out);
+        }
+      else
+        sweep<P1, DIM, 1, false, true>(qt.S, b, out);
+    }
+
+    // compile-time tile shape per (dim, degree, precision); the fallback
+    // shape serves time dimensions whose bricks do not fit the main one
+    template <int DIM, int P, typename T, bool BIG>
+    struct OpShape
+    {
+      static constexpr int TX = DIM == 2 ? (P <= 2 ? (BIG ? 16 : 4) : (P <= 4 ? (BIG ? 8 : 2) : (BIG ? 4 : 1)))
+                                         : (P == 1 ? (BIG ? 8 : 2) : (P == 2 ? (BIG ? (sizeof(T) == 4 ? 8 : 4) : 2) : (BIG ? 4 : 1)));
+      static constexpr int TY = DIM == 2 ? TX : (P == 1 ? TX : (P == 2 ? (BIG ? 4 : 2) : (BIG ? (P == 3 ? 4 : 2) : 1)));
+      static constexpr int TZ = DIM == 2 ? 1 : (P == 1 ? TX : (P == 2 ? (BIG ? 4 : 2) : (BIG ? 2 : 1)));
+    };
+
+
+    // One CTA per tile of cells (persistent over tiles):
+    //  A. the tile's input brick, all time values of a node contiguous, is
+    //     staged by cp.async one tile ahead (Dirichlet and out-of-mesh nodes
+    //     zero); warps walk brick rows, lanes cover (node, time) pairs;
+    //  B. one thread per (output time dof j, cell): a_j = sum_i A(j,i) kappa
+    //     u_i and b_j = sum_i B(j,i) u_i at the cell's nodes (one vector load
+    //     per node), then K a_j + M b_j by register sum factorisation, into
+    //     the per-cell result buffer;
+    //  C. one thread per (j, brick node): the sum over the node's cells in a
+    //     fixed order; tile-interior nodes go to dst, shell nodes to the
+    //     tile's face slots (or constrained writes when one tile covers the
+    //     mesh).
+    // NTPC: 1 or 2 time values per node, or 4 for multiples of four.
+    template <int DIM, int P, typename T, int MODE, int TX, int TY, int TZ, int NTPC>
+    __global__ void __launch_bounds__(256, (sizeof(T) == 4 && MODE == 1) ? 2 : 1)
+    st_apply_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<T> tm,
+                    const __grid_constant__ Cart1D<T> c1, const __grid_constant__ QTab<T> qt,
+                    const T *__restrict__ src, T *__restrict__ dst, T *__restrict__ shell, const OutMode<T> om)
+    {
+      using S          = TileShape<DIM, P, TX, TY, TZ>;
+      constexpr int ND = S::ND;
+      constexpr int P1 = P + 1;
+      constexpr int NW = 8; // warps per CTA
+      extern __shared__ __align__(16) unsigned char smem_raw[];
+      const int nti = tm.nt_in, nto = tm.nt_out;
+      const int ntp = NTPC == 4 ? (nti + 3) / 4 * 4 : NTPC;
+      T        *bricks[2] = {reinterpret_cast<T *>(smem_raw), reinterpret_cast<T *>(smem_raw) + S::NB * ntp};
+      T        *cellbuf   = bricks[1] + S::NB * ntp; // [nto][TC][ND]
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      // brick load lanes: (node along x, time value)
+      const int npl = 32 / ntp, lnode = lane / ntp, li = lane - lnode * ntp;
+      const int n_tiles = int(tl.n_tiles);
+
+      // padded time slots are never loaded: keep them zero
+      for (int idx = threadIdx.x; idx < 2 * S::NB * ntp; idx += blockDim.x)
+        bricks[0][idx] = T(0);
+      __syncthreads();
+
+      auto load = [&](int tile, T *brick) {
+        const int t0 = tile % tl.ntiles[0], t1 = (tile / tl.ntiles[0]) % tl.ntiles[1],
+                  t2 = tile / (tl.ntiles[0] * tl.ntiles[1]);
+        const int gx0 = t0 * tl.T[0] * P, gy0 = t1 * tl.T[1] * P, gz0 = t2 * tl.T[2] * P;
+        const int ex = min(tl.T[0], m.n[0] - t0 * tl.T[0]) * P + 1;
+        const int ey = DIM > 1 ? min(tl.T[1], m.n[1] - t1 * tl.T[1]) * P + 1 : 1;
+        const int ez = DIM == 3 ? min(tl.T[2], m.n[2] - t2 * tl.T[2]) * P + 1 : 1;
+        if (lnode >= npl || li >= nti)
+          return;
+        for (int row = warp; row < S::E1 * S::E2; row += NW)
+          {
+            const int  bz = row / S::E1, by = row - bz * S::E1;
+            const int  gy = gy0 + by, gz = gz0 + bz;
+            bool       rok = by < ey && bz < ez && gy > 0 && gy < m.nn[1] - 1;
+            if (DIM == 3)
+              rok = rok && gz > 0 && gz < m.nn[2] - 1;
+            const T   *grow = src + li * m.N + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+            T         *srow = brick + (long long)row * S::E0 * ntp + li;
+            for (int bx = lnode; bx < S::E0; bx += npl)
+              {
+                const int  gx = gx0 + bx;
+                const bool ok = rok && bx < ex && gx > 0 && gx < m.nn[0] - 1;
+                cp_async_small<sizeof(T)>(srow + bx * ntp, ok ? grow + gx : src, ok);
+              }
+          }
+      };
+
+      int tile = blockIdx.x;
+      if (tile < n_tiles)
+        load(tile, bricks[0]);
+      cp_async_commit();
+      for (int buf = 0; tile < n_tiles; tile += gridDim.x, buf ^= 1)
+        {
+          if (tile + int(gridDim.x) < n_tiles)
+            load(tile + gridDim.x, bricks[buf ^ 1]);
+          cp_async_commit();
+          cp_async_wait<1>();
+          __syncthreads();
+          int t[3], c0[3], tc[3], e[3];
+          tile_extents<DIM>(m, tl, tile, t, c0, tc, e);
+
+          // B. per (output time dof, cell)
+          const T *brick = bricks[buf];
+          for (int w = threadIdx.x; w < nto * S::TC; w += blockDim.x)
+            {
+              const int j = w / S::TC, lc = w - j * S::TC;
+              const int lx = lc % TX, ly = (lc / TX) % TY, lz = lc / (TX * TY);
+              if (lx >= tc[0] || ly >= tc[1] || lz >= tc[2])
+                continue;
+              const int       cx = c0[0] + lx, cy = c0[1] + ly, cz = c0[2] + lz;
+              const long long cell = cx + (long long)m.n[0] * (cy + (long long)m.n[1] * cz);
+              T               kap  = T(1);
+              if (MODE == 1 && m.coeff_mode == 1)
+                kap = sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell]);
+              T a[ND], b[ND];
+#pragma unroll
+              for (int q = 0; q < ND; ++q)
+                a[q] = b[q] = T(0);
+              const T *br0 = brick + (lx * P + S::E0 * (ly * P + S::E1 * (lz * P))) * ntp;
+              for (int i0 = 0; i0 < ntp; i0 += NTPC)
+                {
+                  T al[NTPC], be[NTPC];
+#pragma unroll
+                  for (int u = 0; u < NTPC; ++u)
+                    {
+                      const int i = i0 + u;
+                      al[u]       = i < nti ? tm.A[j * nti + i] * kap : T(0);
+                      be[u]       = i < nti ? tm.B[j * nti + i] : T(0);
+                    }
+#pragma unroll
+                  for (int q = 0; q < ND; ++q)
+                    {
+                      const T *x = br0 + S::offset(q) * ntp + i0;
+                      T        xv[NTPC];
+                      if constexpr (NTPC == 4 && sizeof(T) == 4)
+                        {
+                          const float4 v = *reinterpret_cast<const float4 *>(x);
+                          xv[0] = v.x, xv[1] = v.y, xv[2] = v.z, xv[NTPC - 1] = v.w;
+                        }
+                      else if constexpr (NTPC >= 2)
+                        {
+#pragma unroll
+                          for (int u = 0; u < NTPC; u += 2)
+                            {
+                              if constexpr (sizeof(T) == 8)
+                                {
+                                  const double2 v = *reinterpret_cast<const double2 *>(x + u);
+                                  xv[u] = v.x, xv[u + 1] = v.y;
+                                }
+                              else
+                                {
+                                  const float2 v = *reinterpret_cast<const float2 *>(x + u);
+                                  xv[u] = v.x, xv[u + 1] = v.y;
+                                }
+                            }
+                        }
+                      else
+                        xv[0] = x[0];
+#pragma unroll
+                      for (int u = 0; u < NTPC; ++u)
+                        {
+                          a[q] += al[u] * xv[u];
+                          b[q] += be[u] * xv[u];
+                        }
+                    }
+                }
+              T out[ND];
+              if constexpr (MODE == 1)
+                cart_apply<DIM, P>(c1, a, b, out);
+              else if constexpr (MODE == 2)
+                box_apply<DIM, P>(m, qt, cell, a, b, out);
+              else
+                general_apply<DIM, P>(m, qt, cx, cy, cz, cell, a, b, out);
+              T *cb = cellbuf + (j * S::TC + lc) * ND;
+#pragma unroll
+              for (int q = 0; q < ND; ++q)
+                cb[q] = out[q];
+            }
+          __syncthreads();
+
+          // C. per (j, brick node): sum over the node's cells, write out.
+          // A node on a cell face also belongs to the next cell along that
+          // direction: offsets to the second candidate per direction, and
+          // lane (x) constants for the tile, row (y, z) constants per row.
+          int  lx_base[2], lx_dx[2], lx_two[2];
+          bool lx_in[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+            {
+              const int  bx   = lane + 32 * h;
+              const bool face = bx % P == 0 && bx > 0;
+              const int  cx0  = face ? bx / P - 1 : bx / P;
+              const int  ax0  = face ? P : bx % P;
+              lx_base[h]      = cx0 * ND + ax0;
+              lx_dx[h]        = ND - ax0;
+              lx_two[h]       = face && bx / P < tc[0];
+              lx_in[h]        = bx > 0 && bx < e[0] - 1;
+            }
+          for (int row = warp; row < S::E1 * S::E2; row += NW)
+            {
+              const int bz = row / S::E1, by = row - bz * S::E1;
+              if (by >= e[1] || bz >= e[2])
+                continue;
+              const bool fy = by % P == 0 && by > 0;
+              const int  cy0 = fy ? by / P - 1 : by / P, ay0 = fy ? P : by % P;
+              const bool ty  = fy && by / P < tc[1];
+              const int  dy  = TX * ND - P1 * ay0;
+              int        cz0 = 0, az0 = 0, dz = 0;
+              bool       tz  = false;
+              if (DIM == 3)
+                {
+                  const bool fz = bz % P == 0 && bz > 0;
+                  cz0           = fz ? bz / P - 1 : bz / P;
+                  az0           = fz ? P : bz % P;
+                  tz            = fz && bz / P < tc[2];
+                  dz            = TX * TY * ND - P1 * P1 * az0;
+                }
+              const T   *cbr = cellbuf + TX * (cy0 + TY * cz0) * ND + P1 * (ay0 + P1 * az0);
+              const long long grow = c0[0] * P + (long long)m.nn[0] * ((c0[1] * P + by) + (long long)m.nn[1] * (c0[2] * P + bz));
+              const bool yzin = by > 0 && by < e[1] - 1 && (DIM < 3 || (bz > 0 && bz < e[2] - 1));
+              // shell slot of this row: x faces by (y, z); y and z faces by x
+              long long rslot = 0;
+              if (!yzin)
+                {
+                  if (by == 0)
+                    rslot = tl.face_off[2] + (long long)tl.E[0] * bz;
+                  else if (by == e[1] - 1 || DIM == 2)
+                    rslot = tl.face_off[3] + (long long)tl.E[0] * bz;
+                  else if (bz == 0)
+                    rslot = tl.face_off[4] + (long long)tl.E[0] * by;
+                  else
+                    rslot = tl.face_off[5] + (long long)tl.E[0] * by;
+                }
+              const long long xslot = by + (long long)tl.E[1] * bz;
+#pragma unroll
+              for (int h = 0; h < (S::E0 + 31) / 32; ++h)
+                {
+                  const int bx = lane + 32 * h;
+                  if (bx >= e[0])
+                    break;
+                  const T  *c    = cbr + lx_base[h];
+                  const int dx   = lx_dx[h];
+                  const bool two = lx_two[h];
+                  const long long slot = bx == 0 ? tl.face_off[0] + xslot
+                                                 : (bx == e[0] - 1 ? tl.face_off[1] + xslot : rslot + bx);
+                  const bool inner = yzin && lx_in[h];
+                  const T   *cj    = c;
+                  long long  gj    = grow + bx; // index into dst and rhs
+                  T         *sj    = shell + (long long)tile * nto * tl.tile_stride + slot;
+                  for (int j = 0; j < nto; ++j, cj += S::TC * ND, gj += m.N, sj += tl.tile_stride)
+                    {
+                      T s = cj[0];
+                      if (two)
+                        s += cj[dx];
+                      if (ty)
+                        {
+                          s += cj[dy];
+                          if (two)
+                            s += cj[dy + dx];
+                        }
+                      if (tz)
+                        {
+                          s += cj[dz];
+                          if (two)
+                            s += cj[dz + dx];
+                          if (ty)
+                            {
+                              s += cj[dz + dy];
+                              if (two)
+                                s += cj[dz + dy + dx];
+                            }
+                        }
+                      if (inner)
+                        om.write(dst, gj, s);
+                      else if (tl.n_tiles == 1)
+                        om.write_constrained(dst, gj);
+                      else
+                        *sj = s;
+                    }
+                }
+            }
+          __syncthreads();
+        }
+      cp_async_wait<0>();
+    }
+  } // namespace op_detail
+
+  template <int DIM, int P, typename T, int MODE, bool BIG, int NTPC>
+  void
+  op_launch_variant(const OpLaunch<T> &L)
+  {
+    using Sh = op_detail::OpShape<DIM, P, T, BIG>;
+    auto kern = op_detail::st_apply_kernel<DIM, P, T, MODE, Sh::TX, Sh::TY, Sh::TZ, NTPC>;
+    const int shape[3] = {Sh::TX, Sh::TY, Sh::TZ};
+    const std::size_t smem = op_smem_bytes(DIM, P, shape, L.tm.nt_in, L.tm.nt_out, sizeof(T));
+    const unsigned grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, L.tl.n_tiles);
+    kern<<<grid, 256, smem, L.s>>>(L.m, L.tl, L.tm, L.c1, L.qt, L.src, L.dst, L.shell, L.om);
+    count_launch();
+    STMG_CUDA(cudaGetLastError());
+    if (L.tl.n_tiles > 1)
+      launch_plane_fixup<DIM, T, false>(L.m, L.tl, L.tm.nt_out, L.shell, L.dst, L.om, L.s);
+  }
+
+  template <int DIM, int P, typename T, int MODE, bool BIG>
+  void
+  op_launch_nt(const OpLaunch<T> &L)
+  {
+    const int nti = L.tm.nt_in;
+    if (nti == 1)
+      return op_launch_variant<DIM, P, T, MODE, BIG, 1>(L);
+    if (nti == 2)
+      return op_launch_variant<DIM, P, T, MODE, BIG, 2>(L);
+    return op_launch_variant<DIM, P, T, MODE, BIG, 4>(L);
+  }
+
+  template <int DIM, int P, typename T, int MODE>
+  void
+  op_launch_mode(const OpLaunch<T> &L)
+  {
+    if (L.big)
+      op_launch_nt<DIM, P, T, MODE, true>(L);
+    else
+      op_launch_nt<DIM, P, T, MODE, false>(L);
+  }
+
+  // the dispatch every st_apply_d<D>p<P>.cu instantiates
+  template <int DIM, int P, typename T>
+  void
+  op_launch_impl(const OpLaunch<T> &L)
+  {
+    if (L.m.cartesian)
+      op_launch_mode<DIM, P, T, 1>(L);
+    else if (L.m.box)
+      op_launch_mode<DIM, P, T, 2>(L);
+    else
+      op_launch_mode<DIM, P, T, 0>(L);
+  }
+} // namespace stmg

@@ -1,0 +1,19 @@
+// Space-time operator kernels for 2-D meshes of degree 4.
+#include "op_apply_impl.cuh"
+
+namespace stmg
+{
+  template <>
+  void
+  op_launch_dp<2, 4, float>(const OpLaunch<float> &L)
+  {
+    op_launch_impl<2, 4, float>(L);
+  }
+
+  template <>
+  void
+  op_launch_dp<2, 4, double>(const OpLaunch<double> &L)
+  {
+    op_launch_impl<2, 4, double>(L);
+  }
+} // namespace stmg

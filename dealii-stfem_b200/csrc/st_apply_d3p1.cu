@@ -1,0 +1,19 @@
+// Space-time operator kernels for 3-D meshes of degree 1.
+#include "op_apply_impl.cuh"
+
+namespace stmg
+{
+  template <>
+  void
+  op_launch_dp<3, 1, float>(const OpLaunch<float> &L)
+  {
+    op_launch_impl<3, 1, float>(L);
+  }
+
+  template <>
+  void
+  op_launch_dp<3, 1, double>(const OpLaunch<double> &L)
+  {
+    op_launch_impl<3, 1, double>(L);
+  }
+} // namespace stmg

@@ -1,366 +1,35 @@
 // Fused space-time operator dst_j = sum_i A(j,i) K src_i + B(j,i) M src_i
 // (the reference's SystemMatrix over two MatrixFreeOperator objects,
 // tests/include/operators.h:71-256 and 355-562), one pass over the cells for
-// all time blocks at once.
-//
-// One CTA per tile of cells:
-//  A. stage the tile's node brick of every input time block in shared
-//     memory (Dirichlet nodes read as zero);
-//  B. one thread per (cell, output time dof j): mix the inputs in time at
-//     the nodes, a_j = sum_i A(j,i) kappa u_i and b_j = sum_i B(j,i) u_i, and
-//     form K a_j + M b_j by register-resident sum factorisation (exact 1-D
-//     matrices on cartesian cells, QGauss(p+1) with the Q1 geometry at every
-//     quadrature point otherwise);
-//  C. gather the cell results per brick node in a fixed order; tile-interior
-//     nodes are final and go to dst, brick-shell nodes go to the tile's
-//     face slots, summed by the fix-up kernel in a fixed tile order.
-// The result is deterministic (no atomics) and dst is written exactly once.
+// all time blocks at once: host side (tiling, time matrices, dispatch). The
+// kernels live in op_apply_impl.cuh: per tile of cells the input brick is
+// staged in shared memory, one thread per (output time dof, cell) mixes the
+// time blocks and applies K and M by sum factorisation, and one thread per
+// (time dof, brick node) sums the node's cells in a fixed order; nodes the
+// tiles share go through per-tile face slots summed by the fix-up kernel.
+// The result is deterministic (no atomics).
 #include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
 
+#include "op_apply_impl.cuh"
 #include "st_operator.h"
-#include "tile_ops.cuh"
 
 namespace stmg
 {
   namespace
   {
-    template <int DIM, int P, typename T>
-    __device__ __forceinline__ void
-    cart_apply(const Cart1D<T> &c, T *a, T *b, T *out)
-    {
-      constexpr int P1 = P + 1;
-      constexpr int ND = Tens<P1, DIM>::ND;
-      if constexpr (DIM == 2)
-        {
-          // K a + M b = Kx (My a) + Mx (Ky a + My b)
-          T s[ND];
-          sweep<P1, 2, 1, false, false>(c.M[1], a, s);
-          sweep<P1, 2, 1, false, false>(c.K[1], a, a);
-          sweep<P1, 2, 1, true, false>(c.M[1], b, a);
-          sweep<P1, 2, 0, false, false>(c.K[0], s, out);
-          sweep<P1, 2, 0, true, false>(c.M[0], a, out);
-        }
-      else
-        {
-          // K a + M b = Kx (My Mz a) + Mx (Ky Mz a + My (Kz a + Mz b))
-          T s[ND], u[ND];
-          sweep<P1, 3, 2, false, false>(c.M[2], a, s);
-          sweep<P1, 3, 2, false, false>(c.K[2], a, a);
-          sweep<P1, 3, 2, true, false>(c.M[2], b, a);
-          sweep<P1, 3, 1, false, false>(c.M[1], s, u);
-          sweep<P1, 3, 1, false, false>(c.K[1], s, b);
-          sweep<P1, 3, 1, true, false>(c.M[1], a, b);
-          sweep<P1, 3, 0, false, false>(c.K[0], u, out);
-          sweep<P1, 3, 0, true, false>(c.M[0], b, out);
-        }
-    }
-
-    // K a + M b on a Q1-mapped cell with QGauss(p+1) and a coefficient per
-    // cell or per quadrature point.
-    template <int DIM, int P, typename T>
-    __device__ __forceinline__ void
-    general_apply(const MeshView &m, const QTab<T> &qt, int cx, int cy, int cz, long long cell, T *a, T *b, T *out)
-    {
-      constexpr int P1 = P + 1;
-      constexpr int ND = Tens<P1, DIM>::ND;
-      // values at the quadrature points
-      sweep<P1, DIM, 0, false, false>(qt.S, a, a);
-      sweep<P1, DIM, 1, false, false>(qt.S, a, a);
-      sweep<P1, DIM, 0, false, false>(qt.S, b, b);
-      sweep<P1, DIM, 1, false, false>(qt.S, b, b);
-      if constexpr (DIM == 3)
-        {
-          sweep<P1, DIM, 2, false, false>(qt.S, a, a);
-          sweep<P1, DIM, 2, false, false>(qt.S, b, b);
-        }
-      // reference gradients by collocation
-      T g0[ND], g1[ND], g2[DIM == 3 ? ND : 1];
-      sweep<P1, DIM, 0, false, false>(qt.Dq, a, g0);
-      sweep<P1, DIM, 1, false, false>(qt.Dq, a, g1);
-      if constexpr (DIM == 3)
-        sweep<P1, DIM, 2, false, false>(qt.Dq, a, g2);
-      T X[1 << DIM][DIM];
-      load_corners<DIM>(m, cx, cy, cz, X);
-      const T *cq    = nullptr;
-      T        kcell = T(1);
-      if constexpr (sizeof(T) == 8)
-        {
-          if (m.coeff_mode == 1)
-            kcell = T(m.coeff64[cell]);
-          else if (m.coeff_mode == 2)
-            cq = reinterpret_cast<const T *>(m.coeff64) + cell * ND;
-        }
-      else
-        {
-          if (m.coeff_mode == 1)
-            kcell = T(m.coeff32[cell]);
-          else if (m.coeff_mode == 2)
-            cq = reinterpret_cast<const T *>(m.coeff32) + cell * ND;
-        }
-#pragma unroll
-      for (int q = 0; q < ND; ++q)
-        {
-          const int qx = q % P1, qy = (q / P1) % P1, qz = q / (P1 * P1);
-          T         xi[3] = {qt.gx[qx], qt.gx[qy], DIM == 3 ? qt.gx[qz] : T(0)};
-          T         J[DIM][DIM], Ji[DIM][DIM];
-          q1_jacobian<DIM>(X, xi, J);
-          const T det = det_inv<DIM>(J, Ji);
-          T       w   = qt.gw[qx] * qt.gw[qy];
-          if constexpr (DIM == 3)
-            w *= qt.gw[qz];
-          const T JxW = fabs(det) * w;
-          const T k   = (cq ? cq[q] : kcell) * JxW;
-          // physical gradient Ji^T g, flux = k Ji (Ji^T g)
-          T gr[DIM] = {g0[q], g1[q]};
-          if constexpr (DIM == 3)
-            gr[2] = g2[q];
-          T ph[DIM];
-#pragma unroll
-          for (int i = 0; i < DIM; ++i)
-            {
-              T s = T(0);
-#pragma unroll
-              for (int d = 0; d < DIM; ++d)
-                s += Ji[d][i] * gr[d];
-              ph[i] = k * s;
-            }
-#pragma unroll
-          for (int d = 0; d < DIM; ++d)
-            {
-              T s = T(0);
-#pragma unroll
-              for (int i = 0; i < DIM; ++i)
-                s += Ji[d][i] * ph[i];
-              gr[d] = s;
-            }
-          g0[q] = gr[0];
-          g1[q] = gr[1];
-          if constexpr (DIM == 3)
-            g2[q] = gr[2];
-          b[q] *= JxW;
-        }
-      // integrate: collocation derivatives transposed, then S^T
-      sweep<P1, DIM, 0, true, true>(qt.Dq, g0, b);
-      sweep<P1, DIM, 1, true, true>(qt.Dq, g1, b);
-      if constexpr (DIM == 3)
-        sweep<P1, DIM, 2, true, true>(qt.Dq, g2, b);
-      sweep<P1, DIM, 0, false, true>(qt.S, b, b);
-      sweep<P1, DIM, 1, false, true>(qt.S, b, b);
-      if constexpr (DIM == 3)
-        sweep<P1, DIM, 2, false, true>(qt.S, b, out);
-      else
-#pragma unroll
-        for (int q = 0; q < ND; ++q)
-          out[q] = b[q];
-    }
-
-    // K a + M b on an axis-parallel box cell (Jacobian diag(h)) with a
-    // coefficient per quadrature point: general_apply with the geometry
-    // folded into per-direction constants.
-    template <int DIM, int P, typename T>
-    __device__ __forceinline__ void
-    box_apply(const MeshView &m, const QTab<T> &qt, long long cell, T *a, T *b, T *out)
-    {
-      constexpr int P1 = P + 1;
-      constexpr int ND = Tens<P1, DIM>::ND;
-      sweep<P1, DIM, 0, false, false>(qt.S, a, a);
-      sweep<P1, DIM, 1, false, false>(qt.S, a, a);
-      sweep<P1, DIM, 0, false, false>(qt.S, b, b);
-      sweep<P1, DIM, 1, false, false>(qt.S, b, b);
-      if constexpr (DIM == 3)
-        {
-          sweep<P1, DIM, 2, false, false>(qt.S, a, a);
-          sweep<P1, DIM, 2, false, false>(qt.S, b, b);
-        }
-      T g0[ND], g1[ND], g2[DIM == 3 ? ND : 1];
-      sweep<P1, DIM, 0, false, false>(qt.Dq, a, g0);
-      sweep<P1, DIM, 1, false, false>(qt.Dq, a, g1);
-      if constexpr (DIM == 3)
-        sweep<P1, DIM, 2, false, false>(qt.Dq, a, g2);
-      T det = T(m.h[0]) * T(m.h[1]);
-      if constexpr (DIM == 3)
-        det *= T(m.h[2]);
-      const T ih0 = T(1) / (T(m.h[0]) * T(m.h[0])), ih1 = T(1) / (T(m.h[1]) * T(m.h[1]));
-      const T ih2 = DIM == 3 ? T(1) / (T(m.h[2]) * T(m.h[2])) : T(0);
-      const T *cq = m.coeff_mode == 2 ? (sizeof(T) == 8 ? reinterpret_cast<const T *>(m.coeff64)
-                                                         : reinterpret_cast<const T *>(m.coeff32)) +
-                                          cell * ND
-                                      : nullptr;
-      const T kcell = m.coeff_mode == 1 ? (sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell])) : T(1);
-#pragma unroll
-      for (int q = 0; q < ND; ++q)
-        {
-          const int qx = q % P1, qy = (q / P1) % P1, qz = q / (P1 * P1);
-          T         w  = qt.gw[qx] * qt.gw[qy];
-          if constexpr (DIM == 3)
-            w *= qt.gw[qz];
-          const T JxW = det * w;
-          const T k   = (cq ? cq[q] : kcell) * JxW;
-          g0[q] *= k * ih0;
-          g1[q] *= k * ih1;
-          if constexpr (DIM == 3)
-            g2[q] *= k * ih2;
-          b[q] *= JxW;
-        }
-      sweep<P1, DIM, 0, true, true>(qt.Dq, g0, b);
-      sweep<P1, DIM, 1, true, true>(qt.Dq, g1, b);
-      if constexpr (DIM == 3)
-        sweep<P1, DIM, 2, true, true>(qt.Dq, g2, b);
-      sweep<P1, DIM, 0, false, true>(qt.S, b, b);
-      if constexpr (DIM == 3)
-        {
-          sweep<P1, DIM, 1, false, true>(qt.S, b, b);
-          sweep<P1, DIM, 2, false, true>(qt.S, b, out);
-        }
-      else
-        sweep<P1, DIM, 1, false, true>(qt.S, b, out);
-    }
-
-    // MODE 1: cartesian cells, coefficient per cell (cart_apply); 2: box
-    // cells, coefficient per quadrature point (box_apply); 0: general
-    template <int DIM, int P, typename T, int MODE, int TX, int TY, int TZ>
-    __global__ void __launch_bounds__(256, (sizeof(T) == 4 && MODE == 1) ? 2 : 1)
-    st_apply_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<T> tm,
-                    const __grid_constant__ Cart1D<T> c1, const __grid_constant__ QTab<T> qt,
-                    const T *__restrict__ src, T *__restrict__ dst, T *__restrict__ shell, const OutMode<T> om)
-    {
-      using S          = TileShape<DIM, P, TX, TY, TZ>;
-      constexpr int ND = S::ND;
-      extern __shared__ __align__(16) unsigned char smem_raw[];
-      const int nbuf    = max(tm.nt_in, tm.nt_out) * S::NB;
-      T        *bricks[2] = {reinterpret_cast<T *>(smem_raw), reinterpret_cast<T *>(smem_raw) + nbuf};
-      T        *cellbuf   = bricks[1] + nbuf;
-      long long tile      = blockIdx.x;
-      int       t[3], c0[3], tc[3], e[3];
-      if (tile < tl.n_tiles)
-        {
-          tile_extents<DIM>(m, tl, tile, t, c0, tc, e);
-          load_brick<S>(bricks[0], src, m, tm.nt_in, c0, e);
-        }
-      cp_async_commit();
-      for (int buf = 0; tile < tl.n_tiles; tile += gridDim.x, buf ^= 1)
-        {
-          tile_extents<DIM>(m, tl, tile, t, c0, tc, e);
-          const long long next = tile + gridDim.x;
-          if (next < tl.n_tiles)
-            {
-              int nt3[3], nc0[3], ntc[3], ne[3];
-              tile_extents<DIM>(m, tl, next, nt3, nc0, ntc, ne);
-              load_brick<S>(bricks[buf ^ 1], src, m, tm.nt_in, nc0, ne);
-            }
-          cp_async_commit();
-          cp_async_wait<1>();
-          __syncthreads();
-
-          // B. per (output time dof, cell): K a_j + M b_j into cellbuf
-          const T *brick = bricks[buf];
-          for (int w = threadIdx.x; w < tm.nt_out * S::TC; w += blockDim.x)
-            {
-              const int j = w / S::TC, lc = w - j * S::TC;
-              const int lx = lc % TX, ly = (lc / TX) % TY, lz = lc / (TX * TY);
-              if (lx >= tc[0] || ly >= tc[1] || lz >= tc[2])
-                continue;
-              const int cx = c0[0] + lx, cy = c0[1] + ly, cz = c0[2] + lz;
-              const long long cell = cx + (long long)m.n[0] * (cy + (long long)m.n[1] * cz);
-              T kap = T(1);
-              if (MODE == 1 && m.coeff_mode == 1)
-                kap = sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell]);
-              T a[ND], b[ND];
-#pragma unroll
-              for (int q = 0; q < ND; ++q)
-                a[q] = b[q] = T(0);
-              const T *br0 = brick + lx * P + S::E0 * (ly * P + S::E1 * (lz * P));
-              for (int i = 0; i < tm.nt_in; ++i)
-                {
-                  const T  al = tm.A[j * tm.nt_in + i] * kap, be = tm.B[j * tm.nt_in + i];
-                  const T *br = br0 + i * S::NB;
-                  if (al != T(0))
-#pragma unroll
-                    for (int q = 0; q < ND; ++q)
-                      a[q] += al * br[S::offset(q)];
-                  if (be != T(0))
-#pragma unroll
-                    for (int q = 0; q < ND; ++q)
-                      b[q] += be * br[S::offset(q)];
-                }
-              T out[ND];
-              if constexpr (MODE == 1)
-                cart_apply<DIM, P>(c1, a, b, out);
-              else if constexpr (MODE == 2)
-                box_apply<DIM, P>(m, qt, cell, a, b, out);
-              else
-                general_apply<DIM, P>(m, qt, cx, cy, cz, cell, a, b, out);
-              T *cb = cellbuf + (j * S::TC + lc) * ND;
-#pragma unroll
-              for (int q = 0; q < ND; ++q)
-                cb[q] = out[q];
-            }
-          __syncthreads();
-          // C. coloured scatter into the output brick (the current input
-          // brick's buffer, no longer read), D. write out
-          T *ob = bricks[buf];
-          scatter_cells<S, DIM, T>(cellbuf, ob, tm.nt_out, tc);
-          write_brick<S, DIM, T, false>(ob, m, tl, tile, tm.nt_out, c0, e, dst, shell, om);
-          __syncthreads();
-        }
-      cp_async_wait<0>();
-    }
-
-    // compile-time tile shape per (dim, degree, precision); the fallback
-    // shape serves time dimensions whose bricks do not fit the main one
-    template <int DIM, int P, typename T, bool BIG>
-    struct OpShape
-    {
-      static constexpr int TX = DIM == 2 ? (P <= 2 ? (BIG ? 16 : 4) : (P <= 4 ? (BIG ? 8 : 2) : (BIG ? 4 : 1)))
-                                         : (P == 1 ? (BIG ? 8 : 2) : (P == 2 ? (BIG ? (sizeof(T) == 4 ? 8 : 4) : 2) : (BIG ? 4 : 1)));
-      static constexpr int TY = DIM == 2 ? TX : (P == 1 ? TX : (P == 2 ? (BIG ? 4 : 2) : (BIG ? (P == 3 ? 4 : 2) : 1)));
-      static constexpr int TZ = DIM == 2 ? 1 : (P == 1 ? TX : (P == 2 ? (BIG ? 4 : 2) : (BIG ? 2 : 1)));
-    };
-
-    template <int DIM, int P, typename T, bool BIG>
-    void
-    launch_shape(const StOperator &op, const TimeMats<T> &tm, const T *src, T *dst, T *shell, const OutMode<T> &om,
-                 const Tiling &tl, std::size_t smem, cudaStream_t s)
-    {
-      using Sh = OpShape<DIM, P, T, BIG>;
-      const MeshView &m    = op.mesh->v;
-      auto            kern = m.cartesian ? st_apply_kernel<DIM, P, T, 1, Sh::TX, Sh::TY, Sh::TZ>
-                             : (m.box ? st_apply_kernel<DIM, P, T, 2, Sh::TX, Sh::TY, Sh::TZ>
-                                      : st_apply_kernel<DIM, P, T, 0, Sh::TX, Sh::TY, Sh::TZ>);
-      const unsigned  grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, tl.n_tiles);
-      kern<<<grid, 256, smem, s>>>(m, tl, tm, op.cart<T>(), op.qtab<T>(), src, dst, shell, om);
-      count_launch();
-      STMG_CUDA(cudaGetLastError());
-      if (tl.n_tiles > 1)
-        launch_plane_fixup<DIM, T, false>(m, tl, tm.nt_out, shell, dst, om, s);
-    }
-
-    template <int DIM, int P, typename T>
-    void
-    launch_dp(const StOperator &op, bool transpose, const T *src, T *dst, T *shell, const OutMode<T> &om,
-              cudaStream_t s)
-    {
-      const TimeMats<T> &tm  = transpose ? op.tmT<T>() : op.tm<T>();
-      const bool         big = transpose ? op.bigT : op.big;
-      const Tiling      &tl  = transpose ? op.tilingT : op.tiling;
-      const std::size_t  smem = op.smem_bytes(transpose ? op.shpT : op.shp, tm.nt_in, tm.nt_out, sizeof(T));
-      if (big)
-        launch_shape<DIM, P, T, true>(op, tm, src, dst, shell, om, tl, smem, s);
-      else
-        launch_shape<DIM, P, T, false>(op, tm, src, dst, shell, om, tl, smem, s);
-    }
-
     template <typename T>
     void
     launch(const StOperator &op, bool transpose, const T *src, T *dst, T *shell, const OutMode<T> &om, cudaStream_t s)
     {
+      OpLaunch<T> L{op.mesh->v, transpose ? op.tilingT : op.tiling, transpose ? op.tmT<T>() : op.tm<T>(),
+                    op.cart<T>(), op.qtab<T>(), src, dst, shell, om, transpose ? op.bigT : op.big, s};
       const int dim = op.mesh->v.dim, p = op.mesh->v.p;
 #define STMG_CASE(D, PP)                                                                                 \
   if (dim == D && p == PP)                                                                               \
-    return launch_dp<D, PP, T>(op, transpose, src, dst, shell, om, s);
+    return op_launch_dp<D, PP, T>(L);
       STMG_CASE(2, 1) STMG_CASE(2, 2) STMG_CASE(2, 3) STMG_CASE(2, 4) STMG_CASE(2, 5)
       STMG_CASE(3, 1) STMG_CASE(3, 2) STMG_CASE(3, 3) STMG_CASE(3, 4)
 #undef STMG_CASE
@@ -412,9 +81,9 @@ namespace stmg
   if (dim == D && p == PP)                                                                               \
     {                                                                                                    \
       if (big)                                                                                           \
-        T3[0] = OpShape<D, PP, T, true>::TX, T3[1] = OpShape<D, PP, T, true>::TY, T3[2] = OpShape<D, PP, T, true>::TZ; \
+        T3[0] = op_detail::OpShape<D, PP, T, true>::TX, T3[1] = op_detail::OpShape<D, PP, T, true>::TY, T3[2] = op_detail::OpShape<D, PP, T, true>::TZ; \
       else                                                                                               \
-        T3[0] = OpShape<D, PP, T, false>::TX, T3[1] = OpShape<D, PP, T, false>::TY, T3[2] = OpShape<D, PP, T, false>::TZ; \
+        T3[0] = op_detail::OpShape<D, PP, T, false>::TX, T3[1] = op_detail::OpShape<D, PP, T, false>::TY, T3[2] = op_detail::OpShape<D, PP, T, false>::TZ; \
       return;                                                                                            \
     }
       STMG_SH(2, 1) STMG_SH(2, 2) STMG_SH(2, 3) STMG_SH(2, 4) STMG_SH(2, 5)
@@ -427,12 +96,7 @@ namespace stmg
   std::size_t
   StOperator::smem_bytes(const int *shape, int nt_in_, int nt_out_, std::size_t elem) const
   {
-    // two bricks (each holding the larger of the input and output blocks)
-    // and the per-cell results, for the compile-time tile shape
-    const int         p = mesh->v.p, dim = mesh->v.dim;
-    const std::size_t nb = std::size_t(shape[0] * p + 1) * (shape[1] * p + 1) * (dim == 3 ? shape[2] * p + 1 : 1);
-    const std::size_t tc = std::size_t(shape[0]) * shape[1] * (dim == 3 ? shape[2] : 1);
-    return elem * (2 * std::size_t(std::max(nt_in_, nt_out_)) * nb + tc * nt_out_ * mesh->nd);
+    return op_smem_bytes(mesh->v.dim, mesh->v.p, shape, nt_in_, nt_out_, elem);
   }
 
   Tiling
@@ -571,11 +235,7 @@ namespace stmg
     box_tiling(const MeshView &m, int nd, int nt_in, int nt_out, bool &big_out)
     {
       const std::size_t budget = 200 * 1024;
-      auto              smem   = [&](const int *sh) {
-        const std::size_t nb = std::size_t(sh[0] * m.p + 1) * (sh[1] * m.p + 1) * (m.dim == 3 ? sh[2] * m.p + 1 : 1);
-        const std::size_t tc = std::size_t(sh[0]) * sh[1] * (m.dim == 3 ? sh[2] : 1);
-        return sizeof(T) * (2 * std::size_t(std::max(nt_in, nt_out)) * nb + tc * nt_out * nd);
-      };
+      auto              smem   = [&](const int *sh) { return op_smem_bytes(m.dim, m.p, sh, nt_in, nt_out, sizeof(T)); };
       int big_sh[3], small_sh[3];
       shape_of<T>(m.dim, m.p, true, big_sh);
       shape_of<T>(m.dim, m.p, false, small_sh);
@@ -588,25 +248,6 @@ namespace stmg
       STMG_REQUIRE(small_fits, STMG_ERR_UNSUPPORTED, "operator: time blocks do not fit in shared memory");
       big_out = false;
       return make_tiling(m, small_sh);
-    }
-
-    template <int DIM, int P, typename T, bool BIG>
-    void
-    launch_box(const MeshView &m, const Tiling &tl, const TimeMats<T> &tm, const Cart1D<T> &c1, const QTab<T> &qt,
-               const T *src, T *dst, T *shell, cudaStream_t s)
-    {
-      using Sh = OpShape<DIM, P, T, BIG>;
-      using S  = TileShape<DIM, P, Sh::TX, Sh::TY, Sh::TZ>;
-      const std::size_t smem = sizeof(T) * (2 * std::size_t(std::max(tm.nt_in, tm.nt_out)) * S::NB +
-                                            std::size_t(S::TC) * tm.nt_out * S::ND);
-      auto              kern = st_apply_kernel<DIM, P, T, 1, Sh::TX, Sh::TY, Sh::TZ>;
-      const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, tl.n_tiles);
-      const OutMode<T>  om{T(1), T(0), nullptr};
-      kern<<<grid, 256, smem, s>>>(m, tl, tm, c1, qt, src, dst, shell, om);
-      count_launch();
-      STMG_CUDA(cudaGetLastError());
-      if (tl.n_tiles > 1)
-        launch_plane_fixup<DIM, T, false>(m, tl, tm.nt_out, shell, dst, om, s);
     }
 
     template <typename T>
@@ -630,12 +271,11 @@ namespace stmg
           tm.A[k] = T(A[k]);
           tm.B[k] = T(B[k]);
         }
-      const Cart1D<T> c1 = make_cart<T>(m);
-      const QTab<T>   qt = make_qtab<T>(m.p);
+      const OpLaunch<T> L{m, tl, tm, make_cart<T>(m), make_qtab<T>(m.p), src, dst, shell, OutMode<T>{T(1), T(0), nullptr},
+                          big, s};
 #define STMG_BOX(D, PP)                                                                                  \
   if (m.dim == D && m.p == PP)                                                                           \
-    return big ? launch_box<D, PP, T, true>(m, tl, tm, c1, qt, src, dst, shell, s)                       \
-               : launch_box<D, PP, T, false>(m, tl, tm, c1, qt, src, dst, shell, s);
+    return op_launch_dp<D, PP, T>(L);
       STMG_BOX(2, 1) STMG_BOX(2, 2) STMG_BOX(2, 3) STMG_BOX(2, 4) STMG_BOX(2, 5)
       STMG_BOX(3, 1) STMG_BOX(3, 2) STMG_BOX(3, 3) STMG_BOX(3, 4)
 #undef STMG_BOX

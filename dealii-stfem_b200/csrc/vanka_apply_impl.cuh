@@ -594,36 +594,45 @@ namespace stmg
             {
               __syncthreads();
               // the tile's output: interior nodes -> dst (1/valence), shell
-              // nodes -> face slots (or constrained writes for one tile)
-              const int gx   = tg.c0[0] * P + lx;
-              const int vx   = (gx % P == 0) ? 2 : 1;
+              // nodes -> face slots (or constrained writes for one tile);
+              // warps walk (y, z) rows, lanes x, the time dofs innermost
+              const int  gx  = tg.c0[0] * P + lx;
+              const int  vx  = (gx % P == 0) ? 2 : 1;
               const bool inx = lx > 0 && lx < tg.e[0] - 1;
-              for (int rb = warp * RPW; rb < ROWS; rb += NW * RPW)
+              for (int rb = warp * RPW; rb < S::E1 * S::E2; rb += NW * RPW)
                 {
                   const int row = rb + lrow;
-                  if (lrow >= RPW || row >= ROWS || lx >= tg.e[0])
+                  if (lrow >= RPW || row >= S::E1 * S::E2 || lx >= tg.e[0])
                     continue;
-                  const int j = row / (S::E1 * S::E2), rem = row - j * (S::E1 * S::E2);
-                  const int bz = rem / S::E1, by = rem - bz * S::E1;
+                  const int bz = row / S::E1, by = row - bz * S::E1;
                   if (by >= tg.e[1] || bz >= tg.e[2])
                     continue;
-                  const float sv   = bout[((bz * S::E1 + by) * S::E0 + lx) * NTP + j];
-                  bool        inte = inx && by > 0 && by < tg.e[1] - 1;
+                  bool inte = inx && by > 0 && by < tg.e[1] - 1;
                   if (DIM == 3)
                     inte = inte && bz > 0 && bz < tg.e[2] - 1;
-                  const int       gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
-                  const long long gi = j * m.N + gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+                  const int gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
+                  int       v  = vx * ((gy % P == 0) ? 2 : 1);
+                  if (DIM == 3)
+                    v *= (gz % P == 0) ? 2 : 1;
+                  const float w = v == 1 ? 1.0f : (v == 2 ? 0.5f : (v == 4 ? 0.25f : 0.125f));
+                  float       o[NT];
+                  TV::load(bout + ((bz * S::E1 + by) * S::E0 + lx) * NTP, o);
+                  long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
                   if (inte)
-                    {
-                      int v = vx * ((gy % P == 0) ? 2 : 1);
-                      if (DIM == 3)
-                        v *= (gz % P == 0) ? 2 : 1;
-                      om.write(dst, gi, sv * (v == 1 ? 1.0f : (v == 2 ? 0.5f : (v == 4 ? 0.25f : 0.125f))));
-                    }
+#pragma unroll
+                    for (int j = 0; j < NT; ++j, gi += m.N)
+                      om.write(dst, gi, o[j] * w);
                   else if (tl.n_tiles == 1)
-                    om.write_constrained(dst, gi);
+#pragma unroll
+                    for (int j = 0; j < NT; ++j, gi += m.N)
+                      om.write_constrained(dst, gi);
                   else
-                    shell[((long long)tile * NT + j) * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz)] = sv;
+                    {
+                      float *sj = shell + (long long)tile * NT * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz);
+#pragma unroll
+                      for (int j = 0; j < NT; ++j, sj += tl.tile_stride)
+                        *sj = o[j];
+                    }
                 }
               __syncthreads();
               for (int idx = threadIdx.x; idx < S::NB * NTP; idx += blockDim.x)
