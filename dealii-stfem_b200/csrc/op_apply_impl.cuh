@@ -197,21 +197,16 @@ namespace stmg
           sweep<P1, DIM, 2, false, false>(qt.S, a, a);
           sweep<P1, DIM, 2, false, false>(qt.S, b, b);
         }
-      T g0[ND], g1[ND], g2[DIM == 3 ? ND : 1];
-      sweep<P1, DIM, 0, false, false>(qt.Dq, a, g0);
-      sweep<P1, DIM, 1, false, false>(qt.Dq, a, g1);
-      if constexpr (DIM == 3)
-        sweep<P1, DIM, 2, false, false>(qt.Dq, a, g2);
       T det = T(m.h[0]) * T(m.h[1]);
       if constexpr (DIM == 3)
         det *= T(m.h[2]);
-      const T ih0 = T(1) / (T(m.h[0]) * T(m.h[0])), ih1 = T(1) / (T(m.h[1]) * T(m.h[1]));
-      const T ih2 = DIM == 3 ? T(1) / (T(m.h[2]) * T(m.h[2])) : T(0);
       const T *cq = m.coeff_mode == 2 ? (sizeof(T) == 8 ? reinterpret_cast<const T *>(m.coeff64)
                                                          : reinterpret_cast<const T *>(m.coeff32)) +
                                           cell * ND
                                       : nullptr;
       const T kcell = m.coeff_mode == 1 ? (sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell])) : T(1);
+      // coefficient x JxW at the quadrature points (kept in a), mass part in b
+      T kw[ND];
 #pragma unroll
       for (int q = 0; q < ND; ++q)
         {
@@ -220,17 +215,31 @@ namespace stmg
           if constexpr (DIM == 3)
             w *= qt.gw[qz];
           const T JxW = det * w;
-          const T k   = (cq ? cq[q] : kcell) * JxW;
-          g0[q] *= k * ih0;
-          g1[q] *= k * ih1;
-          if constexpr (DIM == 3)
-            g2[q] *= k * ih2;
+          kw[q]       = (cq ? cq[q] : kcell) * JxW;
           b[q] *= JxW;
         }
-      sweep<P1, DIM, 0, true, true>(qt.Dq, g0, b);
-      sweep<P1, DIM, 1, true, true>(qt.Dq, g1, b);
-      if constexpr (DIM == 3)
-        sweep<P1, DIM, 2, true, true>(qt.Dq, g2, b);
+      // one gradient component at a time: b += Dq_d^T (k JxW / h_d^2 Dq_d a)
+      T g[ND];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+        {
+          const T ih = T(1) / (T(m.h[d]) * T(m.h[d]));
+          if (d == 0)
+            sweep<P1, DIM, 0, false, false>(qt.Dq, a, g);
+          else if (d == 1)
+            sweep<P1, DIM, 1, false, false>(qt.Dq, a, g);
+          else
+            sweep<P1, DIM, DIM == 3 ? 2 : 1, false, false>(qt.Dq, a, g);
+#pragma unroll
+          for (int q = 0; q < ND; ++q)
+            g[q] *= kw[q] * ih;
+          if (d == 0)
+            sweep<P1, DIM, 0, true, true>(qt.Dq, g, b);
+          else if (d == 1)
+            sweep<P1, DIM, 1, true, true>(qt.Dq, g, b);
+          else
+            sweep<P1, DIM, DIM == 3 ? 2 : 1, true, true>(qt.Dq, g, b);
+        }
       sweep<P1, DIM, 0, false, true>(qt.S, b, b);
       if constexpr (DIM == 3)
         {
@@ -247,8 +256,8 @@ namespace stmg
     struct OpShape
     {
       static constexpr int TX = DIM == 2 ? (P <= 2 ? (BIG ? 16 : 4) : (P <= 4 ? (BIG ? 8 : 2) : (BIG ? 4 : 1)))
-                                         : (P == 1 ? (BIG ? 8 : 2) : (P == 2 ? (BIG ? (sizeof(T) == 4 ? 8 : 4) : 2) : (BIG ? 4 : 1)));
-      static constexpr int TY = DIM == 2 ? TX : (P == 1 ? TX : (P == 2 ? (BIG ? 4 : 2) : (BIG ? (P == 3 ? 4 : 2) : 1)));
+                                         : (P == 1 ? (BIG ? 8 : 2) : (P == 2 ? (BIG ? (sizeof(T) == 4 ? 8 : 4) : 4) : (BIG ? 4 : 1)));
+      static constexpr int TY = DIM == 2 ? TX : (P == 1 ? TX : (P == 2 ? 4 : (BIG ? (P == 3 ? 4 : 2) : 1)));
       static constexpr int TZ = DIM == 2 ? 1 : (P == 1 ? TX : (P == 2 ? (BIG ? 4 : 2) : (BIG ? 2 : 1)));
     };
 
@@ -267,7 +276,7 @@ namespace stmg
     //     mesh).
     // NTPC: 1 or 2 time values per node, or 4 for multiples of four.
     template <int DIM, int P, typename T, int MODE, int TX, int TY, int TZ, int NTPC>
-    __global__ void __launch_bounds__(256, (sizeof(T) == 4 && MODE == 1) ? 2 : 1)
+    __global__ void __launch_bounds__(256, (sizeof(T) == 4 && MODE != 0) ? 2 : 1)
     st_apply_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<T> tm,
                     const __grid_constant__ Cart1D<T> c1, const __grid_constant__ QTab<T> qt,
                     const T *__restrict__ src, T *__restrict__ dst, T *__restrict__ shell, const OutMode<T> om)

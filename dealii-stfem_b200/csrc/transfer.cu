@@ -3,8 +3,8 @@
 //     block, and its transpose (deal.II's MGTwoLevelTransfer as wrapped by
 //     MGTwoLevelBlockTransfer, tests/include/gmg.h:35-75); on a structured
 //     mesh the global prolongation is the tensor product of 1-D stencils, so
-//     both directions run in gather form (one thread per output node, fixed
-//     summation order, Dirichlet nodes zero on both sides).
+//     both directions run tile by tile in shared memory, one direction at a
+//     time (fixed summation order, Dirichlet nodes zero on both sides).
 //  t: (P (x) I) over the time blocks (MGTwoLevelTransferST::prolongate_and_add
 //     / restrict_and_add, gmg.h:121-135, via tensorproduct_add,
 //     operators.h:46-58).
@@ -18,123 +18,6 @@ namespace stmg
 {
   namespace
   {
-    template <typename T>
-    __global__ void
-    h_prolongate_kernel(const MeshView fm, const MeshView cm, int nt, const int *__restrict__ start,
-                        const double *__restrict__ w, const T *__restrict__ src, T *__restrict__ dst)
-    {
-      const long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-      if (node >= fm.N)
-        return;
-      const int g[3] = {int(node % fm.nn[0]), int((node / fm.nn[0]) % fm.nn[1]), int(node / ((long long)fm.nn[0] * fm.nn[1]))};
-      if (is_boundary_node(fm, g[0], g[1], g[2]))
-        return;
-      const int p1 = fm.p + 1;
-      // 1-D stencils: coarse nodes start[d][g_d] .. +p with weights
-      int    s[3], cnt[3];
-      const double *wd[3];
-      long long off = 0;
-      for (int d = 0; d < 3; ++d)
-        {
-          if (d < fm.dim)
-            {
-              s[d]   = start[off + g[d]];
-              wd[d]  = w + (off + g[d]) * p1;
-              cnt[d] = p1;
-              off += fm.nn[d];
-            }
-          else
-            {
-              s[d]   = 0;
-              wd[d]  = nullptr;
-              cnt[d] = 1;
-            }
-        }
-      for (int j = 0; j < nt; ++j)
-        {
-          T acc = T(0);
-          for (int kz = 0; kz < cnt[2]; ++kz)
-            {
-              const double wz = wd[2] ? wd[2][kz] : 1.0;
-              if (wz == 0.0)
-                continue;
-              for (int ky = 0; ky < cnt[1]; ++ky)
-                {
-                  const double wy = wd[1][ky] * wz;
-                  if (wy == 0.0)
-                    continue;
-                  for (int kx = 0; kx < cnt[0]; ++kx)
-                    {
-                      const double wx = wd[0][kx] * wy;
-                      if (wx == 0.0)
-                        continue;
-                      const int cx = s[0] + kx, cy = s[1] + ky, cz = s[2] + kz;
-                      if (is_boundary_node(cm, cx, cy, cz))
-                        continue;
-                      acc += T(wx) * src[j * cm.N + cx + (long long)cm.nn[0] * (cy + (long long)cm.nn[1] * cz)];
-                    }
-                }
-            }
-          dst[j * fm.N + node] += acc;
-        }
-    }
-
-    template <typename T>
-    __global__ void
-    h_restrict_kernel(const MeshView fm, const MeshView cm, int nt, int maxr, const int *__restrict__ cnt,
-                      const int *__restrict__ fidx, const double *__restrict__ w, const T *__restrict__ src,
-                      T *__restrict__ dst)
-    {
-      const long long node = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-      if (node >= cm.N)
-        return;
-      const int c[3] = {int(node % cm.nn[0]), int((node / cm.nn[0]) % cm.nn[1]), int(node / ((long long)cm.nn[0] * cm.nn[1]))};
-      if (is_boundary_node(cm, c[0], c[1], c[2]))
-        return;
-      int           n[3];
-      const int    *f[3];
-      const double *wd[3];
-      long long     off = 0;
-      for (int d = 0; d < 3; ++d)
-        {
-          if (d < cm.dim)
-            {
-              n[d]  = cnt[off + c[d]];
-              f[d]  = fidx + (off + c[d]) * maxr;
-              wd[d] = w + (off + c[d]) * maxr;
-              off += cm.nn[d];
-            }
-          else
-            {
-              n[d]  = 1;
-              f[d]  = nullptr;
-              wd[d] = nullptr;
-            }
-        }
-      for (int j = 0; j < nt; ++j)
-        {
-          T acc = T(0);
-          for (int kz = 0; kz < n[2]; ++kz)
-            {
-              const int    fz = f[2] ? f[2][kz] : 0;
-              const double wz = wd[2] ? wd[2][kz] : 1.0;
-              for (int ky = 0; ky < n[1]; ++ky)
-                {
-                  const int    fy = f[1][ky];
-                  const double wy = wd[1][ky] * wz;
-                  for (int kx = 0; kx < n[0]; ++kx)
-                    {
-                      const int fx = f[0][kx];
-                      if (is_boundary_node(fm, fx, fy, fz))
-                        continue;
-                      acc += T(wd[0][kx] * wy) * src[j * fm.N + fx + (long long)fm.nn[0] * (fy + (long long)fm.nn[1] * fz)];
-                    }
-                }
-            }
-          dst[j * cm.N + node] += acc;
-        }
-    }
-
     template <typename T>
     __global__ void
     time_transfer_kernel(long long N, int n_out, int n_in, const __grid_constant__ TimeMats<T> P,
@@ -158,6 +41,222 @@ namespace stmg
           dst[i * N + node] = acc;
         }
     }
+
+    // ---------------------------------------------------- tiled h transfer
+    // coarse cells per tile and direction
+    template <int DIM, int P, typename T>
+    constexpr int h_tile_cells()
+    {
+      return DIM == 3 ? (P == 1 ? 8 : (P == 2 ? (sizeof(T) == 4 ? 4 : 2) : 2))
+                      : (P <= 2 ? 32 / (2 * P) : (P == 3 ? 5 : (P == 4 ? 4 : 3)));
+    }
+
+    // Prolongation dst_f += P src_c, one CTA per tile of C^dim coarse cells:
+    // the coarse block (P C + 1 nodes per direction, Dirichlet nodes zero) is
+    // interpolated direction by direction in shared memory (x, then y, then
+    // z) and the fine nodes the tile owns are added to dst (Dirichlet nodes
+    // skipped). Fine nodes [2PC t, 2PC (t+1)) belong to tile t; the last fine
+    // node to the last tile.
+    template <int DIM, int P, int C, typename T>
+    __global__ void __launch_bounds__(256)
+    h_prolongate_tiled(const MeshView fm, const MeshView cm, int nt, const __grid_constant__ HWeights<T> W,
+                       const T *__restrict__ src, T *__restrict__ dst)
+    {
+      constexpr int LC = P * C + 1, LF = 2 * P * C + 1;
+      constexpr int NZC = DIM == 3 ? LC : 1, NZF = DIM == 3 ? LF : 1;
+      __shared__ T sc[NZC * LC * LC], s1[NZC * LC * LF], s2[NZC * LF * LF];
+      const int ntx = (cm.n[0] + C - 1) / C, nty = (cm.n[1] + C - 1) / C;
+      const int tile = blockIdx.x;
+      const int t0 = tile % ntx, t1 = (tile / ntx) % nty, t2 = DIM == 3 ? tile / (ntx * nty) : 0;
+      const int q0[3] = {t0 * C * P, t1 * C * P, t2 * C * P};        // first coarse node
+      const int f0[3] = {2 * t0 * C * P, 2 * t1 * C * P, 2 * t2 * C * P}; // first fine node
+      for (int j = 0; j < nt; ++j)
+        {
+          for (int i = threadIdx.x; i < NZC * LC * LC; i += blockDim.x)
+            {
+              const int x = i % LC, y = (i / LC) % LC, z = i / (LC * LC);
+              const int g[3] = {q0[0] + x, q0[1] + y, DIM == 3 ? q0[2] + z : 0};
+              bool      ok   = g[0] < cm.nn[0] && g[1] < cm.nn[1] && (DIM < 3 || g[2] < cm.nn[2]);
+              ok             = ok && !is_boundary_node(cm, g[0], g[1], g[2]);
+              sc[i] = ok ? src[j * cm.N + g[0] + (long long)cm.nn[0] * (g[1] + (long long)cm.nn[1] * g[2])] : T(0);
+            }
+          __syncthreads();
+          // x: sc[z][y][cx] -> s1[z][y][fx]
+          for (int i = threadIdx.x; i < NZC * LC * LF; i += blockDim.x)
+            {
+              const int fx = i % LF, r = i / LF;
+              const int cc = min(fx / (2 * P), C - 1), t = fx - 2 * P * cc;
+              const T  *in = sc + r * LC + P * cc;
+              T         v  = T(0);
+#pragma unroll
+              for (int b = 0; b <= P; ++b)
+                v += W.w[t][b] * in[b];
+              s1[i] = v;
+            }
+          __syncthreads();
+          // y: s1[z][cy][fx] -> s2[z][fy][fx]
+          for (int i = threadIdx.x; i < NZC * LF * LF; i += blockDim.x)
+            {
+              const int fx = i % LF, fy = (i / LF) % LF, z = i / (LF * LF);
+              const int cc = min(fy / (2 * P), C - 1), t = fy - 2 * P * cc;
+              const T  *in = s1 + (z * LC + P * cc) * LF + fx;
+              T         v  = T(0);
+#pragma unroll
+              for (int b = 0; b <= P; ++b)
+                v += W.w[t][b] * in[b * LF];
+              s2[i] = v;
+            }
+          __syncthreads();
+          // z (3-D): s2[cz][fy][fx] -> fine, added to dst
+          for (int i = threadIdx.x; i < NZF * LF * LF; i += blockDim.x)
+            {
+              const int fx = i % LF, fy = (i / LF) % LF, fz = i / (LF * LF);
+              const int g[3] = {f0[0] + fx, f0[1] + fy, DIM == 3 ? f0[2] + fz : 0};
+              // owned: below the next tile's first node, or the mesh's last node
+              bool own = (fx < LF - 1 || g[0] == fm.nn[0] - 1) && (fy < LF - 1 || g[1] == fm.nn[1] - 1);
+              if (DIM == 3)
+                own = own && (fz < LF - 1 || g[2] == fm.nn[2] - 1);
+              own = own && g[0] < fm.nn[0] && g[1] < fm.nn[1] && (DIM < 3 || g[2] < fm.nn[2]);
+              if (!own || is_boundary_node(fm, g[0], g[1], g[2]))
+                continue;
+              T v;
+              if constexpr (DIM == 3)
+                {
+                  const int cc = min(fz / (2 * P), C - 1), t = fz - 2 * P * cc;
+                  const T  *in = s2 + (P * cc) * LF * LF + fy * LF + fx;
+                  v            = T(0);
+#pragma unroll
+                  for (int b = 0; b <= P; ++b)
+                    v += W.w[t][b] * in[b * LF * LF];
+                }
+              else
+                v = s2[i];
+              dst[j * fm.N + g[0] + (long long)fm.nn[0] * (g[1] + (long long)fm.nn[1] * g[2])] += v;
+            }
+          __syncthreads();
+        }
+    }
+
+    // Restriction dst_c += P^T src_f, one CTA per tile of C^dim coarse cells
+    // owning coarse nodes [PC t, PC (t+1)) (the last node to the last tile):
+    // the fine block [2P(C t - 1), 2P C (t+1)] per direction (Dirichlet and
+    // outside nodes zero) is reduced direction by direction. A coarse vertex
+    // collects the fine nodes of both neighbouring coarse cells, the shared
+    // fine vertex once.
+    template <int DIM, int P, int C, typename T>
+    __global__ void __launch_bounds__(256)
+    h_restrict_tiled(const MeshView fm, const MeshView cm, int nt, const __grid_constant__ HWeights<T> W,
+                     const T *__restrict__ src, T *__restrict__ dst)
+    {
+      constexpr int LR = 2 * P * (C + 1) + 1, LQ = P * C + 1;
+      constexpr int NZR = DIM == 3 ? LR : 1, NZQ = DIM == 3 ? LQ : 1;
+      extern __shared__ __align__(16) unsigned char hr_smem[];
+      T *sf = reinterpret_cast<T *>(hr_smem);
+      T *s1 = sf + NZR * LR * LR;   // [z][y][qx]
+      T *s2 = s1 + NZR * LR * LQ;   // [z][qy][qx]
+      const int ntx = (cm.n[0] + C - 1) / C, nty = (cm.n[1] + C - 1) / C;
+      const int tile = blockIdx.x;
+      const int t0 = tile % ntx, t1 = (tile / ntx) % nty, t2 = DIM == 3 ? tile / (ntx * nty) : 0;
+      const int q0[3] = {t0 * C * P, t1 * C * P, t2 * C * P};
+      const int fo[3] = {2 * P * (t0 * C - 1), 2 * P * (t1 * C - 1), 2 * P * (t2 * C - 1)};
+      // one direction of P^T: out[q] from in[f], stride s between fine entries
+      auto reduce1 = [&](const T *in, int stride, int qx) {
+        const int cl = qx / P, k = qx - P * cl; // coarse cell (local) and index in it
+        T         v  = T(0);
+        // the cell to the right of / containing the node: fine t = 0..2P
+        const T *r = in + (2 * P * (cl + 1)) * stride;
+#pragma unroll
+        for (int t = 0; t <= 2 * P; ++t)
+          v += W.w[t][k] * r[t * stride];
+        if (k == 0)
+          {
+            // the cell to the left: fine t = 0..2P-1
+            const T *l = in + (2 * P * cl) * stride;
+#pragma unroll
+            for (int t = 0; t < 2 * P; ++t)
+              v += W.w[t][P] * l[t * stride];
+          }
+        return v;
+      };
+      for (int j = 0; j < nt; ++j)
+        {
+          for (int i = threadIdx.x; i < NZR * LR * LR; i += blockDim.x)
+            {
+              const int x = i % LR, y = (i / LR) % LR, z = i / (LR * LR);
+              const int g[3] = {fo[0] + x, fo[1] + y, DIM == 3 ? fo[2] + z : 0};
+              bool      ok   = g[0] >= 0 && g[1] >= 0 && g[0] < fm.nn[0] && g[1] < fm.nn[1];
+              if (DIM == 3)
+                ok = ok && g[2] >= 0 && g[2] < fm.nn[2];
+              ok    = ok && !is_boundary_node(fm, g[0], g[1], g[2]);
+              sf[i] = ok ? src[j * fm.N + g[0] + (long long)fm.nn[0] * (g[1] + (long long)fm.nn[1] * g[2])] : T(0);
+            }
+          __syncthreads();
+          for (int i = threadIdx.x; i < NZR * LR * LQ; i += blockDim.x)
+            {
+              const int qx = i % LQ, r = i / LQ;
+              s1[i]        = reduce1(sf + r * LR, 1, qx);
+            }
+          __syncthreads();
+          for (int i = threadIdx.x; i < NZR * LQ * LQ; i += blockDim.x)
+            {
+              const int qx = i % LQ, qy = (i / LQ) % LQ, z = i / (LQ * LQ);
+              s2[i]        = reduce1(s1 + z * LR * LQ + qx, LQ, qy);
+            }
+          __syncthreads();
+          for (int i = threadIdx.x; i < NZQ * LQ * LQ; i += blockDim.x)
+            {
+              const int qx = i % LQ, qy = (i / LQ) % LQ, qz = i / (LQ * LQ);
+              const int g[3] = {q0[0] + qx, q0[1] + qy, DIM == 3 ? q0[2] + qz : 0};
+              bool own = (qx < LQ - 1 || g[0] == cm.nn[0] - 1) && (qy < LQ - 1 || g[1] == cm.nn[1] - 1);
+              if (DIM == 3)
+                own = own && (qz < LQ - 1 || g[2] == cm.nn[2] - 1);
+              own = own && g[0] < cm.nn[0] && g[1] < cm.nn[1] && (DIM < 3 || g[2] < cm.nn[2]);
+              if (!own || is_boundary_node(cm, g[0], g[1], g[2]))
+                continue;
+              const T v = DIM == 3 ? reduce1(s2 + qy * LQ + qx, LQ * LQ, qz) : s2[i];
+              dst[j * cm.N + g[0] + (long long)cm.nn[0] * (g[1] + (long long)cm.nn[1] * g[2])] += v;
+            }
+          __syncthreads();
+        }
+    }
+
+    template <int DIM, int P, typename T>
+    void
+    h_tiled_launch(bool prolong, const MeshView &f, const MeshView &c, int nt, const HWeights<T> &W, const T *src,
+                   T *dst, cudaStream_t s)
+    {
+      constexpr int C = h_tile_cells<DIM, P, T>();
+      long long     tiles = 1;
+      for (int d = 0; d < DIM; ++d)
+        tiles *= (c.n[d] + C - 1) / C;
+      if (prolong)
+        h_prolongate_tiled<DIM, P, C, T><<<unsigned(tiles), 256, 0, s>>>(f, c, nt, W, src, dst);
+      else
+        {
+          constexpr int LR = 2 * P * (C + 1) + 1, LQ = P * C + 1, NZR = DIM == 3 ? LR : 1;
+          const std::size_t smem = sizeof(T) * (std::size_t(NZR) * LR * LR + std::size_t(NZR) * LR * LQ +
+                                                std::size_t(NZR) * LQ * LQ);
+          auto kern = h_restrict_tiled<DIM, P, C, T>;
+          STMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+          kern<<<unsigned(tiles), 256, smem, s>>>(f, c, nt, W, src, dst);
+        }
+      count_launch();
+      STMG_CUDA(cudaGetLastError());
+    }
+
+    template <typename T>
+    void
+    h_tiled(bool prolong, const MeshView &f, const MeshView &c, int nt, const HWeights<T> &W, const T *src, T *dst,
+            cudaStream_t s)
+    {
+#define STMG_HT(D, PP)                                                                                   \
+  if (f.dim == D && f.p == PP)                                                                           \
+    return h_tiled_launch<D, PP, T>(prolong, f, c, nt, W, src, dst, s);
+      STMG_HT(2, 1) STMG_HT(2, 2) STMG_HT(2, 3) STMG_HT(2, 4) STMG_HT(2, 5)
+      STMG_HT(3, 1) STMG_HT(3, 2) STMG_HT(3, 3) STMG_HT(3, 4)
+#undef STMG_HT
+      throw Error(STMG_ERR_UNSUPPORTED, "h-transfer: unsupported dim/degree");
+    }
   } // namespace
 
   HTransfer::HTransfer(Mesh *fine_, Mesh *coarse_, int nt_, int dtype_)
@@ -173,79 +272,46 @@ namespace stmg
     STMG_REQUIRE(nt >= 1 && nt <= MAX_NT, STMG_ERR_ARG, "h-transfer: time blocks 1..16");
     const FETables &t  = host_tables();
     const int       p  = f.p, p1 = p + 1;
-    maxr                = 4 * p + 1;
-    std::vector<int>    start, cnt, fidx;
-    std::vector<double> w, rw;
-    for (int d = 0; d < f.dim; ++d)
+    // 1-D weights of the coarse basis at the fine nodes of a coarse cell
+    std::memset(&w64, 0, sizeof(w64));
+    std::memset(&w32, 0, sizeof(w32));
+    for (int tpos = 0; tpos <= 2 * p; ++tpos)
       {
-        // coarse node -> list of (fine node, weight)
-        std::vector<std::vector<std::pair<int, double>>> col(c.nn[d]);
-        for (int g = 0; g < f.nn[d]; ++g)
+        const int    half = tpos > p ? 1 : (tpos == p ? 1 : 0);
+        const int    a    = tpos - half * p;
+        const double xi   = 0.5 * (half + t.xs[p][a]);
+        for (int b = 0; b < p1; ++b)
           {
-            const int    fc = std::min(g / p, f.n[d] - 1);
-            const int    a  = g - fc * p;
-            const int    cc = fc / 2;
-            const double xi = 0.5 * ((fc % 2) + t.xs[p][a]);
-            start.push_back(cc * p);
-            for (int b = 0; b < p1; ++b)
-              {
-                double v = 1.0;
-                for (int k = 0; k < p1; ++k)
-                  if (k != b)
-                    v *= (xi - t.xs[p][k]) / (t.xs[p][b] - t.xs[p][k]);
-                if (std::abs(v) < 1e-14)
-                  v = 0.0;
-                w.push_back(v);
-                if (v != 0.0)
-                  col[cc * p + b].emplace_back(g, v);
-              }
-          }
-        for (int i = 0; i < c.nn[d]; ++i)
-          {
-            STMG_REQUIRE(int(col[i].size()) <= maxr, STMG_ERR_SHAPE, "h-transfer: stencil overflow");
-            cnt.push_back(int(col[i].size()));
-            for (int k = 0; k < maxr; ++k)
-              {
-                fidx.push_back(k < int(col[i].size()) ? col[i][k].first : 0);
-                rw.push_back(k < int(col[i].size()) ? col[i][k].second : 0.0);
-              }
+            double v = 1.0;
+            for (int k = 0; k < p1; ++k)
+              if (k != b)
+                v *= (xi - t.xs[p][k]) / (t.xs[p][b] - t.xs[p][k]);
+            if (std::abs(v) < 1e-14)
+              v = 0.0;
+            w64.w[tpos][b] = v;
+            w32.w[tpos][b] = float(v);
           }
       }
-    p_start.upload(start);
-    p_w.upload(w);
-    r_cnt.upload(cnt);
-    r_f.upload(fidx);
-    r_w.upload(rw);
   }
 
   void
   HTransfer::prolongate_add(const void *src, void *dst, cudaStream_t s) const
   {
     const MeshView &f = fine->v, &c = coarse->v;
-    const unsigned  nb = unsigned((f.N + 255) / 256);
     if (dtype == STMG_F64)
-      h_prolongate_kernel<double><<<nb, 256, 0, s>>>(f, c, nt, p_start.ptr, p_w.ptr, static_cast<const double *>(src),
-                                                     static_cast<double *>(dst));
+      h_tiled<double>(true, f, c, nt, hw<double>(), static_cast<const double *>(src), static_cast<double *>(dst), s);
     else
-      h_prolongate_kernel<float><<<nb, 256, 0, s>>>(f, c, nt, p_start.ptr, p_w.ptr, static_cast<const float *>(src),
-                                                    static_cast<float *>(dst));
-    count_launch();
-    STMG_CUDA(cudaGetLastError());
+      h_tiled<float>(true, f, c, nt, hw<float>(), static_cast<const float *>(src), static_cast<float *>(dst), s);
   }
 
   void
   HTransfer::restrict_add(const void *src, void *dst, cudaStream_t s) const
   {
     const MeshView &f = fine->v, &c = coarse->v;
-    const unsigned  nb = unsigned((c.N + 255) / 256);
     if (dtype == STMG_F64)
-      h_restrict_kernel<double><<<nb, 256, 0, s>>>(f, c, nt, maxr, r_cnt.ptr, r_f.ptr, r_w.ptr,
-                                                   static_cast<const double *>(src), static_cast<double *>(dst));
+      h_tiled<double>(false, f, c, nt, hw<double>(), static_cast<const double *>(src), static_cast<double *>(dst), s);
     else
-      h_restrict_kernel<float><<<nb, 256, 0, s>>>(f, c, nt, maxr, r_cnt.ptr, r_f.ptr, r_w.ptr,
-                                                  static_cast<const float *>(src), static_cast<float *>(dst));
-    count_launch();
-    STMG_CUDA(cudaGetLastError());
+      h_tiled<float>(false, f, c, nt, hw<float>(), static_cast<const float *>(src), static_cast<float *>(dst), s);
   }
 
   TTransfer::TTransfer(Mesh *mesh_, int nt_fine_, int nt_coarse_, const double *P_, const double *R_, int dtype_)

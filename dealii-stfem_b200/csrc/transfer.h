@@ -16,6 +16,15 @@ namespace stmg
     virtual void restrict_add(const void *src, void *dst, cudaStream_t s) const = 0;
   };
 
+  // 1-D weights of the coarse cell's Lagrange basis at the fine nodes inside
+  // it: w[t][b], t = 0..2P (fine position, (fine cell half) * P + local
+  // index), b = 0..P (coarse local node). Kernel parameter.
+  template <typename T>
+  struct HWeights
+  {
+    T w[2 * MAX_P + 1][MAX_P + 1];
+  };
+
   class HTransfer final : public Transfer
   {
   public:
@@ -24,9 +33,17 @@ namespace stmg
     void restrict_add(const void *src, void *dst, cudaStream_t s) const override;
 
     Mesh          *fine, *coarse;
-    int            nt, dtype, maxr = 0;
-    DevBuf<int>    p_start, r_cnt, r_f;
-    DevBuf<double> p_w, r_w;
+    int            nt, dtype;
+    HWeights<double> w64;
+    HWeights<float>  w32;
+    template <typename T>
+    const HWeights<T> &hw() const
+    {
+      if constexpr (sizeof(T) == 8)
+        return w64;
+      else
+        return w32;
+    }
   };
 
   class TTransfer final : public Transfer
