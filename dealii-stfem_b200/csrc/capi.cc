@@ -510,6 +510,18 @@ extern "C"
   }
 
   int
+  stmg_solver_gradient(stmg_solver_t solver, int n_slabs, const double *u_obs, int checkpoint_every, double *misfit,
+                       double *grad, int *its_fwd, int *its_adj, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_gradient: null handle");
+      STMG_REQUIRE(u_obs && grad && misfit, STMG_ERR_ARG, "solver_gradient: null argument");
+      *misfit = solver->s->gradient(n_slabs, u_obs, checkpoint_every, grad, its_fwd, its_adj,
+                                    static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
   stmg_gmg_vmult(stmg_solver_t solver, double *dst, const double *src, void *stream)
   {
     return guard([&] {

@@ -5,6 +5,7 @@
 #include <cstring>
 
 #include "kernels_common.cuh"
+#include "op_apply_impl.cuh"
 #include "solver.h"
 
 namespace stmg
@@ -12,6 +13,102 @@ namespace stmg
   namespace
   {
     constexpr double PI = 3.14159265358979323846;
+
+    // ------------------------------------------------- adjoint gradient
+    // g[c] += scale * kappa_c * sum_j lam_j^T K_c (sum_i T(j,i) V_i) on the
+    // cell's dofs, K_c the cell stiffness with unit coefficient (Dirichlet
+    // dofs excluded): the derivative of lam^T (T (x) K(kappa)) V with respect
+    // to log kappa_c. One thread per cell, FP64.
+    template <int DIM, int P, bool CART>
+    __global__ void
+    grad_contract_kernel(const MeshView m, const __grid_constant__ Cart1D<double> c1,
+                         const __grid_constant__ QTab<double> qt, const __grid_constant__ TimeMats<double> Tm,
+                         const double *__restrict__ lam, const double *__restrict__ V, double scale,
+                         double *__restrict__ g)
+    {
+      constexpr int   P1   = P + 1;
+      constexpr int   ND   = Tens<P1, DIM>::ND;
+      const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+      if (cell >= m.ncells)
+        return;
+      const int cx = int(cell % m.n[0]), cy = int((cell / m.n[0]) % m.n[1]),
+                cz = DIM == 3 ? int(cell / ((long long)m.n[0] * m.n[1])) : 0;
+      long long idx[ND];
+      bool      fr[ND];
+#pragma unroll
+      for (int q = 0; q < ND; ++q)
+        {
+          const int gx = cx * P + q % P1, gy = cy * P + (q / P1) % P1, gz = DIM == 3 ? cz * P + q / (P1 * P1) : 0;
+          idx[q]       = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+          fr[q]        = !is_boundary_node(m, gx, gy, gz);
+        }
+      MeshView mu   = m;
+      mu.coeff_mode = 0; // unit coefficient inside the cell kernels
+      double acc    = 0;
+      for (int j = 0; j < Tm.nt_out; ++j)
+        {
+          double w[ND], z[ND], out[ND];
+#pragma unroll
+          for (int q = 0; q < ND; ++q)
+            {
+              double s = 0;
+              for (int i = 0; i < Tm.nt_in; ++i)
+                s += Tm.A[j * Tm.nt_in + i] * (fr[q] ? V[i * m.N + idx[q]] : 0.0);
+              w[q] = s;
+              z[q] = 0;
+            }
+          if constexpr (CART)
+            op_detail::cart_apply<DIM, P>(c1, w, z, out);
+          else
+            op_detail::general_apply<DIM, P>(mu, qt, cx, cy, cz, cell, w, z, out);
+#pragma unroll
+          for (int q = 0; q < ND; ++q)
+            if (fr[q])
+              acc += lam[j * m.N + idx[q]] * out[q];
+        }
+      const double kap = m.coeff_mode == 1 ? m.coeff64[cell] : 1.0;
+      g[cell] += scale * kap * acc;
+    }
+
+    void
+    grad_contract(const Mesh &mesh, const tfe::Mat &T, const double *lam, const double *V, double scale, double *g,
+                  cudaStream_t s)
+    {
+      const MeshView  &m = mesh.v;
+      TimeMats<double> tm{};
+      tm.nt_out = T.m;
+      tm.nt_in  = T.n;
+      for (int k = 0; k < T.m * T.n; ++k)
+        tm.A[k] = T.a[k];
+      Cart1D<double> c1{};
+      {
+        const FETables &t = host_tables();
+        const int       n = m.p + 1;
+        for (int d = 0; d < 3; ++d)
+          for (int a = 0; a < n; ++a)
+            for (int b = 0; b < n; ++b)
+              {
+                c1.M[d][a * n + b] = t.M1[m.p][a][b] * m.h[d];
+                c1.K[d][a * n + b] = t.K1[m.p][a][b] / m.h[d];
+              }
+      }
+      const QTab<double> qt = make_qtab<double>(m.p);
+      const unsigned     nb = unsigned((m.ncells + 127) / 128);
+#define STMG_GC(D, PP)                                                                                   \
+  if (m.dim == D && m.p == PP)                                                                           \
+    {                                                                                                    \
+      if (m.box)                                                                                         \
+        grad_contract_kernel<D, PP, true><<<nb, 128, 0, s>>>(m, c1, qt, tm, lam, V, scale, g);           \
+      else                                                                                               \
+        grad_contract_kernel<D, PP, false><<<nb, 128, 0, s>>>(m, c1, qt, tm, lam, V, scale, g);          \
+      count_launch();                                                                                    \
+      STMG_CUDA(cudaGetLastError());                                                                     \
+      return;                                                                                            \
+    }
+      STMG_GC(2, 1) STMG_GC(2, 2) STMG_GC(2, 3) STMG_GC(3, 1) STMG_GC(3, 2) STMG_GC(3, 3)
+#undef STMG_GC
+      throw Error(STMG_ERR_UNSUPPORTED, "gradient: dim/degree not supported");
+    }
 
     // ------------------------------------------------- dense tail helpers
     // Device FP64 matrices, column-major: M(i, j) = m[i + j * rows].
@@ -325,7 +422,7 @@ namespace stmg
   }
 
   // ---------------------------------------------------------------- GMG
-  GMG::GMG(const SolverConfig &c, std::vector<std::unique_ptr<Mesh>> &meshes, Blas &b)
+  GMG::GMG(const SolverConfig &c, std::vector<std::unique_ptr<Mesh>> &meshes, Blas &b, bool transpose_time)
     : dtype(c.mg_dtype)
     , cfg(c)
     , blas(b)
@@ -359,6 +456,15 @@ namespace stmg
         lv.nt      = (type == tfe::DG ? r + 1 : r) * ns;
         lv.A       = w[l][0];
         lv.B       = w[l][1];
+        if (transpose_time)
+          for (tfe::Mat *M : {&lv.A, &lv.B})
+            {
+              tfe::Mat t(M->n, M->m);
+              for (int i = 0; i < M->m; ++i)
+                for (int j = 0; j < M->n; ++j)
+                  t(j, i) = (*M)(i, j);
+              *M = t;
+            }
       }
     const std::size_t elem = dtype == STMG_F64 ? 8 : 4;
     for (int l = 0; l < L; ++l)
@@ -813,6 +919,8 @@ namespace stmg
         rK      = type == tfe::CGP ? wn[2] : tfe::Mat(nb, 1);
         rM      = type == tfe::CGP ? wn[3] : wn[2];
       }
+    lhsK_ = lhsK;
+    rK_   = rK;
     A64   = std::make_unique<StOperator>(fine, nb, nb, lhsK.a.data(), lhsM.a.data(), STMG_F64);
     rhs64 = std::make_unique<StOperator>(fine, nb, 1, rK.a.data(), rM.a.data(), STMG_F64);
     if (c.problem == 2)
@@ -1017,6 +1125,96 @@ namespace stmg
         time += cfg.n_steps * cfg.tau;
       }
     STMG_CUDA(cudaStreamSynchronize(s));
+  }
+
+  double
+  SlabSolver::gradient(int n_slabs, const double *obs, int checkpoint_every, double *grad, int *its_fwd, int *its_adj,
+                       cudaStream_t s)
+  {
+    STMG_REQUIRE(cfg.problem == 1, STMG_ERR_UNSUPPORTED, "gradient: heat problems only");
+    STMG_REQUIRE(n_slabs >= 1 && obs && grad, STMG_ERR_ARG, "gradient: bad arguments");
+    Mesh           &fine = *meshes.back();
+    STMG_REQUIRE(fine.v.coeff_mode != 2, STMG_ERR_UNSUPPORTED, "gradient: needs a coefficient per cell");
+    const long long n    = N * nb;
+    const int       k    = checkpoint_every > 0 ? checkpoint_every
+                                                : std::max(1, int(std::ceil(std::sqrt(double(n_slabs)))));
+    const int       nseg = (n_slabs + k - 1) / k;
+    if (!gmgT)
+      gmgT = std::make_unique<GMG>(cfg, meshes, blas, true);
+    DevBuf<double> O(n), d(n), lam(n), lam_next(n), radj(n), g(fine.v.ncells), ck(std::size_t(nseg) * N),
+      U(std::size_t(k) * n), e(N);
+    std::vector<double> ck_time(nseg);
+    STMG_CUDA(cudaMemsetAsync(g.ptr, 0, fine.v.ncells * 8, s));
+    auto load_obs = [&](int slab) {
+      STMG_CUDA(cudaMemcpyAsync(O.ptr, obs + std::size_t(slab) * n, n * 8, cudaMemcpyHostToDevice, s));
+    };
+    auto set_state = [&](const double *u_end, double t) {
+      STMG_CUDA(cudaMemcpyAsync(x.ptr + (nb - 1) * N, u_end, N * 8, cudaMemcpyDeviceToDevice, s));
+      time = t;
+    };
+    // forward: checkpoints (end value of the previous slab) and the misfit
+    double J = 0;
+    for (int slab = 0; slab < n_slabs; ++slab)
+      {
+        if (slab % k == 0)
+          {
+            STMG_CUDA(cudaMemcpyAsync(ck.ptr + std::size_t(slab / k) * N, x.ptr + (nb - 1) * N, N * 8,
+                                      cudaMemcpyDeviceToDevice, s));
+            ck_time[slab / k] = time;
+          }
+        int it = 0;
+        run(1, &it, s);
+        if (its_fwd)
+          its_fwd[slab] = it;
+        load_obs(slab);
+        STMG_CUDA(cudaMemcpyAsync(d.ptr, x.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
+        axpby<double>(n, -1.0, O.ptr, 1.0, d.ptr, s);
+        J += 0.5 * blas.dot<double>(n, d.ptr, d.ptr, s);
+      }
+    // state after the forward run, restored at the end
+    DevBuf<double> x_end(n);
+    STMG_CUDA(cudaMemcpyAsync(x_end.ptr, x.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
+    const double t_end = time;
+    auto         AT    = [&](double *dst, const double *src) { A64->apply(true, src, dst, false, s); };
+    auto         PT    = [&](double *dst, const double *src) { gmgT->vmult(dst, src, s); };
+    bool         have_next = false;
+    for (int seg = nseg - 1; seg >= 0; --seg)
+      {
+        const int s0 = seg * k, s1 = std::min(n_slabs, s0 + k);
+        // recompute the segment's slabs from its checkpoint
+        set_state(ck.ptr + std::size_t(seg) * N, ck_time[seg]);
+        for (int slab = s0; slab < s1; ++slab)
+          {
+            run(1, nullptr, s);
+            STMG_CUDA(cudaMemcpyAsync(U.ptr + std::size_t(slab - s0) * n, x.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
+          }
+        for (int slab = s1 - 1; slab >= s0; --slab)
+          {
+            const double *Us = U.ptr + std::size_t(slab - s0) * n;
+            // adjoint rhs: U_s - O_s + E^T R^T lambda_{s+1}
+            load_obs(slab);
+            STMG_CUDA(cudaMemcpyAsync(radj.ptr, Us, n * 8, cudaMemcpyDeviceToDevice, s));
+            axpby<double>(n, -1.0, O.ptr, 1.0, radj.ptr, s);
+            if (have_next)
+              rhs64->apply(true, lam_next.ptr, radj.ptr + (nb - 1) * N, true, s);
+            STMG_CUDA(cudaMemsetAsync(lam.ptr, 0, n * 8, s));
+            const int it = gmres->solve(AT, PT, lam.ptr, radj.ptr, cfg.abs_tol, cfg.tol, cfg.max_iter, s);
+            if (its_adj)
+              its_adj[slab] = it;
+            // gradient: lambda_s^T (rK (x) K_c) e(U_{s-1}) - lambda_s^T (Alpha (x) K_c) U_s
+            grad_contract(fine, lhsK_, lam.ptr, Us, -1.0, g.ptr, s);
+            const double *prev = slab == s0 ? ck.ptr + std::size_t(seg) * N
+                                            : U.ptr + std::size_t(slab - 1 - s0) * n + (nb - 1) * N;
+            grad_contract(fine, rK_, lam.ptr, prev, 1.0, g.ptr, s);
+            std::swap(lam.ptr, lam_next.ptr);
+            have_next = true;
+          }
+      }
+    STMG_CUDA(cudaMemcpyAsync(x.ptr, x_end.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
+    time = t_end;
+    STMG_CUDA(cudaMemcpyAsync(grad, g.ptr, fine.v.ncells * 8, cudaMemcpyDeviceToHost, s));
+    STMG_CUDA(cudaStreamSynchronize(s));
+    return J;
   }
 
   void

@@ -48,7 +48,10 @@ namespace stmg
   class GMG
   {
   public:
-    GMG(const SolverConfig &cfg, std::vector<std::unique_ptr<Mesh>> &meshes, Blas &blas);
+    // transpose_time: every level uses Alpha^T, Beta^T (the preconditioner
+    // of the adjoint system A^T)
+    GMG(const SolverConfig &cfg, std::vector<std::unique_ptr<Mesh>> &meshes, Blas &blas,
+        bool transpose_time = false);
     ~GMG();
     GMG(const GMG &)            = delete;
     GMG &operator=(const GMG &) = delete;
@@ -122,6 +125,14 @@ namespace stmg
     int  solve(double *x, const double *rhs, cudaStream_t s);
     void system_vmult(double *dst, const double *src, cudaStream_t s);
     void download(double *u, double *v) const;
+    // Heat only: runs n_slabs slabs from the current state and returns the
+    // misfit J = 1/2 sum_s |U_s - O_s|^2 (obs: host, n_slabs x n_t x N) and
+    // dJ/d(log kappa_c) per fine cell (grad: host), by the discrete adjoint
+    // run backward over the slabs (A^T lambda_s = U_s - O_s + E^T R^T
+    // lambda_{s+1}); forward states are kept every `checkpoint_every` slabs
+    // and recomputed segment by segment. Leaves the state after the last slab.
+    double gradient(int n_slabs, const double *obs, int checkpoint_every, double *grad, int *its_fwd,
+                    int *its_adj, cudaStream_t s);
 
     SolverConfig                        cfg;
     std::vector<std::unique_ptr<Mesh>>  meshes; // coarsest first
@@ -136,6 +147,8 @@ namespace stmg
     tfe::Mat                            AixB, AixG, AixZ;
     DevBuf<double>                      x, v, prev_x, prev_v, rhs, F, Mf, fsrc;
     std::vector<double>                 node_x; // node coordinates (host), N x dim
+    tfe::Mat                            lhsK_, rK_; // time matrices of K in the system and the rhs
+    std::unique_ptr<GMG>                gmgT;       // preconditioner of A^T (built on first use)
     std::vector<int>                    last_iterations;
 
   private:

@@ -287,6 +287,23 @@ class Solver:
                                       _stream(stream)))
         return k.value
 
+    def gradient(self, u_obs, n_slabs=None, checkpoint_every=0, stream=None):
+        """Misfit J = 1/2 sum_s |U_s - O_s|^2 of the next n_slabs slabs and
+        dJ/dlog(kappa) per fine cell by the adjoint slab sweep
+        (stmg_solver_gradient). u_obs: (n_slabs, n_blocks * n_nodes)."""
+        obs = np.ascontiguousarray(u_obs, dtype=np.float64).reshape(-1)
+        if n_slabs is None:
+            n_slabs = obs.size // (self.n_blocks * self.n_nodes)
+        assert obs.size == n_slabs * self.n_blocks * self.n_nodes
+        ncells = int(np.prod([s << self.cfg.refine for s in list(self.cfg.subdiv)[:self.cfg.dim]]))
+        grad = np.zeros(ncells)
+        J = C.c_double()
+        itf = np.zeros(n_slabs, dtype=np.int32)
+        ita = np.zeros(n_slabs, dtype=np.int32)
+        check(lib().stmg_solver_gradient(self.h, n_slabs, _ptr(obs), checkpoint_every, C.byref(J), _ptr(grad),
+                                         itf.ctypes.data_as(_ip), ita.ctypes.data_as(_ip), _stream(stream)))
+        return J.value, grad, itf, ita
+
     def gmg_vmult(self, dst, src, stream=None):
         check(lib().stmg_gmg_vmult(self.h, _dev(dst), _dev(src), _stream(stream)))
 

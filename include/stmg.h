@@ -188,6 +188,19 @@ STMG_API int stmg_solver_solution(stmg_solver_t solver, double *u, double *v);
 /* SolverFGMRES::solve of the slab system (time_integrators.h:174) on device
  * vectors x (initial guess in, solution out) and rhs */
 STMG_API int stmg_solver_solve(stmg_solver_t solver, double *x, const double *rhs, int *iterations, void *stream);
+/* Adjoint gradient (heat): runs n_slabs slabs from the current state and
+ * returns the space-time misfit J = 1/2 sum_s |U_s - O_s|^2 over all slab
+ * time dofs and nodes (u_obs: host, n_slabs x n_t x N, slab-major) and dJ/d
+ * log(kappa_c) for every fine cell (grad: host, n_cells doubles; the solver's
+ * fine coefficient is kappa). The adjoint slab equations A^T lambda_s =
+ * U_s - O_s + E^T R^T lambda_{s+1} run backward over the slabs through a
+ * multigrid built on the transposed time matrices (SystemMatrix::Tvmult,
+ * operators.h:124-152); forward states are kept every checkpoint_every slabs
+ * (<= 0: ceil(sqrt(n_slabs))) and recomputed per segment. its_fwd, its_adj
+ * (host, n_slabs each, may be NULL) receive the FGMRES iterations. The
+ * solver's state afterwards is the state after the last slab. */
+STMG_API int stmg_solver_gradient(stmg_solver_t solver, int n_slabs, const double *u_obs, int checkpoint_every,
+                                  double *misfit, double *grad, int *its_fwd, int *its_adj, void *stream);
 /* GMG::vmult (gmg.h:846-859) on FP64 device vectors */
 STMG_API int stmg_gmg_vmult(stmg_solver_t solver, double *dst, const double *src, void *stream);
 /* the FP64 slab system SystemMatrix::vmult (operators.h:94-122) */
