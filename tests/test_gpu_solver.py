@@ -112,3 +112,53 @@ def test_dense_tail_matches_sweeps(monkeypatch, dim, refine, k, steps, mg):
         b.gmg_vmult(yb, x)
     torch.cuda.synchronize()
     assert torch.linalg.norm(ya - yb) <= tol * torch.linalg.norm(yb)
+
+
+def test_gpu_distorted_q3_matches_oracle():
+    """The 32^3 Q3 distorted-mesh configuration scaled down: 4^3 Q3 cells,
+    interior vertices moved by up to 0.2 h per axis, per-cell coefficient
+    10^U(-2, 2), f = 1 (nodal), dG(2); GPU and oracle (both FP32 V-cycle)."""
+    import stmg
+    R, n = 2, 4
+    X = meshes.vertices(3, (n, n, n), distort=0.2, seed=21)
+    coeff = meshes.log_uniform(n ** 3, 1e-2, 1e2, seed=22)
+    f = np.ones((3 * n + 1) ** 3)
+    kw = dict(dim=3, refine=R, r=2, problem=orc.HEAT, n_steps=1, tau=1 / 32, n_slabs=2, rhs_mode=1)
+    ref = orc.run(p=3, ttype=orc.DG, f_nodal=f, fine_coeff=coeff, fine_vertices=X, compute_errors=False, tol=1e-10,
+                  abs_tol=1e-14, **kw)
+    s = stmg.Solver(dim=3, refine=R, degree=3, time_degree=2, time_type=stmg.DG, problem=stmg.HEAT, n_steps=1,
+                    tau=1 / 32, rhs_mode=1, f_nodal=f, fine_coeff=coeff, fine_vertices=X, tol=1e-10, abs_tol=1e-14)
+    its = s.run(2)
+    assert np.all(np.abs(its - ref["iterations"]) <= 1), (its, ref["iterations"])
+    u, _ = s.solution()
+    assert np.linalg.norm(u - ref["u"]) <= 1e-7 * np.linalg.norm(ref["u"])
+
+
+def test_gpu_wave_bf16_vanka_keeps_iterations():
+    """The wave configuration's precision question scaled down (4^3 Q2
+    cells, dG(2), c^2 in {0.5, 1, 4} per cell, Gaussian pulse u0, v0 = 0,
+    f = 0): BF16-stored Vanka eigenvectors vs FP32-stored, same FP64 FGMRES
+    tolerance; iterations within one per slab and solutions within the
+    solver tolerance."""
+    import stmg
+    R, n = 2, 4
+    rng = np.random.default_rng(23)
+    c2 = rng.choice([0.5, 1.0, 4.0], size=n ** 3)
+    kw = dict(dim=3, refine=R, degree=2, time_degree=2, time_type=stmg.DG, problem=stmg.WAVE, n_steps=1,
+              tau=1 / 128, rhs_mode=2, fine_coeff=c2, tol=1e-10, abs_tol=1e-14)
+    nn1 = 2 * n + 1
+    g = np.linspace(0, 1, nn1)
+    Z, Y, Xc = np.meshgrid(g, g, g, indexing="ij")
+    u0 = np.exp(-((Xc - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2) / 0.01).reshape(-1)
+    u0[meshes.boundary_mask(3, (n, n, n), 2)] = 0.0
+    out = {}
+    for st in (stmg.F32, stmg.BF16):
+        s = stmg.Solver(vanka_storage=st, **kw)
+        s.set_initial(u0, np.zeros_like(u0))
+        its = s.run(4)
+        u, _ = s.solution()
+        out[st] = (its, u)
+    its32, u32 = out[stmg.F32]
+    its16, u16 = out[stmg.BF16]
+    assert np.all(np.abs(its16 - its32) <= 1), (its16, its32)
+    assert np.linalg.norm(u16 - u32) <= 1e-7 * np.linalg.norm(u32)
