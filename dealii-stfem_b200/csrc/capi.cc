@@ -1,5 +1,6 @@
 // extern "C" entry points of libstmg_cuda.so (declared in include/stmg.h).
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -506,6 +507,18 @@ extern "C"
       const int k = solver->s->solve(x, rhs, static_cast<cudaStream_t>(stream));
       if (iterations)
         *iterations = k;
+    });
+  }
+
+  int
+  stmg_solver_errors(stmg_solver_t solver, double *linf, double *l2, double *h1)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_errors: null handle");
+      STMG_REQUIRE(linf && l2 && h1, STMG_ERR_ARG, "solver_errors: null argument");
+      *linf = solver->s->err_l8;
+      *l2   = std::sqrt(solver->s->err_l2sq);
+      *h1   = std::sqrt(solver->s->err_h1sq);
     });
   }
 

@@ -14,6 +14,151 @@ namespace stmg
   {
     constexpr double PI = 3.14159265358979323846;
 
+    // ------------------------------------------------- error norms
+    // ErrorCalculator (exact_solution.h:217-299): at one time point the
+    // difference between the FE function and the manufactured solution
+    // u = sin(2 pi f t) prod_i sin(2 pi f x_i), integrated per cell with
+    // QGauss(nq) per direction on the Q1-mapped cell: L2^2, H1-seminorm^2
+    // and the largest |e| at the quadrature points.
+    struct ErrTab
+    {
+      int    nq, p1;
+      double gx[MAX_P + 2], gw[MAX_P + 2];
+      double phi[MAX_P + 2][MAX_P + 1], dphi[MAX_P + 2][MAX_P + 1];
+    };
+
+    template <int DIM>
+    __global__ void
+    err_cell_kernel(const MeshView m, const __grid_constant__ ErrTab et, const double *__restrict__ u, double t,
+                    double f, double *__restrict__ cl2, double *__restrict__ ch1, double *__restrict__ cl8)
+    {
+      const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+      if (cell >= m.ncells)
+        return;
+      const int cx = int(cell % m.n[0]), cy = int((cell / m.n[0]) % m.n[1]),
+                cz = DIM == 3 ? int(cell / ((long long)m.n[0] * m.n[1])) : 0;
+      double X[1 << DIM][DIM];
+      load_corners<DIM>(m, cx, cy, cz, X);
+      const int p = m.p, p1 = et.p1, nq = et.nq;
+      const int nqt = DIM == 3 ? nq * nq * nq : nq * nq, nd = DIM == 3 ? p1 * p1 * p1 : p1 * p1;
+      const double tv = sin(2 * 3.14159265358979323846 * f * t), k2 = 2 * 3.14159265358979323846 * f;
+      double s2 = 0, sh = 0, s8 = 0;
+      for (int q = 0; q < nqt; ++q)
+        {
+          const int qi[3] = {q % nq, (q / nq) % nq, DIM == 3 ? q / (nq * nq) : 0};
+          double    xi[3] = {et.gx[qi[0]], et.gx[qi[1]], DIM == 3 ? et.gx[qi[2]] : 0.0};
+          double    w     = et.gw[qi[0]] * et.gw[qi[1]] * (DIM == 3 ? et.gw[qi[2]] : 1.0);
+          double    J[DIM][DIM], Ji[DIM][DIM];
+          q1_jacobian<DIM>(X, xi, J);
+          const double det = det_inv<DIM>(J, Ji);
+          double       x[DIM];
+#pragma unroll
+          for (int d = 0; d < DIM; ++d)
+            x[d] = 0;
+#pragma unroll
+          for (int v = 0; v < (1 << DIM); ++v)
+            {
+              double wv = 1;
+#pragma unroll
+              for (int e = 0; e < DIM; ++e)
+                wv *= ((v >> e) & 1) ? xi[e] : 1.0 - xi[e];
+#pragma unroll
+              for (int d = 0; d < DIM; ++d)
+                x[d] += wv * X[v][d];
+            }
+          double uh = 0, gr[DIM];
+#pragma unroll
+          for (int d = 0; d < DIM; ++d)
+            gr[d] = 0;
+          for (int a = 0; a < nd; ++a)
+            {
+              const int ai[3] = {a % p1, (a / p1) % p1, DIM == 3 ? a / (p1 * p1) : 0};
+              const int gx = cx * p + ai[0], gy = cy * p + ai[1], gz = DIM == 3 ? cz * p + ai[2] : 0;
+              if (is_boundary_node(m, gx, gy, gz))
+                continue; // the FE function is zero on Dirichlet nodes
+              const double ua = u[gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz)];
+              double       phi = 1, dphi[DIM];
+#pragma unroll
+              for (int d = 0; d < DIM; ++d)
+                dphi[d] = 1;
+#pragma unroll
+              for (int d = 0; d < DIM; ++d)
+                {
+                  const double sv = et.phi[qi[d]][ai[d]];
+                  phi *= sv;
+#pragma unroll
+                  for (int j = 0; j < DIM; ++j)
+                    dphi[j] *= j == d ? et.dphi[qi[d]][ai[d]] : sv;
+                }
+              uh += ua * phi;
+#pragma unroll
+              for (int j = 0; j < DIM; ++j)
+                gr[j] += ua * dphi[j];
+            }
+          double ue = tv, ge[DIM];
+#pragma unroll
+          for (int i = 0; i < DIM; ++i)
+            {
+              ue *= sin(k2 * x[i]);
+              ge[i] = k2 * tv;
+#pragma unroll
+              for (int j = 0; j < DIM; ++j)
+                ge[i] *= i == j ? cos(k2 * x[j]) : sin(k2 * x[j]);
+            }
+          const double e   = uh - ue;
+          const double JxW = fabs(det) * w;
+          s2 += JxW * e * e;
+          s8 = fmax(s8, fabs(e));
+#pragma unroll
+          for (int i = 0; i < DIM; ++i)
+            {
+              double gp = 0;
+#pragma unroll
+              for (int j = 0; j < DIM; ++j)
+                gp += Ji[j][i] * gr[j];
+              sh += JxW * (gp - ge[i]) * (gp - ge[i]);
+            }
+        }
+      cl2[cell] = s2;
+      ch1[cell] = sh;
+      cl8[cell] = s8;
+    }
+
+    // out = {sum a, sum b, max c} over n cells; one block, fixed order
+    __global__ void
+    err_reduce_kernel(long long n, const double *__restrict__ a, const double *__restrict__ b,
+                      const double *__restrict__ c, double *__restrict__ out)
+    {
+      __shared__ double sa[1024], sb[1024], sc[1024];
+      double            x = 0, y = 0, z = 0;
+      for (long long i = threadIdx.x; i < n; i += blockDim.x)
+        {
+          x += a[i];
+          y += b[i];
+          z = fmax(z, c[i]);
+        }
+      sa[threadIdx.x] = x;
+      sb[threadIdx.x] = y;
+      sc[threadIdx.x] = z;
+      __syncthreads();
+      for (int h = blockDim.x / 2; h > 0; h >>= 1)
+        {
+          if (threadIdx.x < h)
+            {
+              sa[threadIdx.x] += sa[threadIdx.x + h];
+              sb[threadIdx.x] += sb[threadIdx.x + h];
+              sc[threadIdx.x] = fmax(sc[threadIdx.x], sc[threadIdx.x + h]);
+            }
+          __syncthreads();
+        }
+      if (threadIdx.x == 0)
+        {
+          out[0] = sa[0];
+          out[1] = sb[0];
+          out[2] = sc[0];
+        }
+    }
+
     // ------------------------------------------------- adjoint gradient
     // g[c] += scale * kappa_c * sum_j lam_j^T K_c (sum_i T(j,i) V_i) on the
     // cell's dofs, K_c the cell stiffness with unit coefficient (Dirichlet
@@ -1014,7 +1159,8 @@ namespace stmg
     STMG_CUDA(cudaMemcpy(x.ptr + (nb - 1) * N, hu.data(), N * 8, cudaMemcpyHostToDevice));
     if (cfg.problem == 2)
       STMG_CUDA(cudaMemcpy(v.ptr + (nb - 1) * N, hv.data(), N * 8, cudaMemcpyHostToDevice));
-    time = 0;
+    time     = 0;
+    err_l2sq = err_h1sq = err_l8 = 0;
   }
 
   void
@@ -1122,9 +1268,92 @@ namespace stmg
                   }
               }
           }
+        if (cfg.rhs_mode == 0)
+          accumulate_errors(tq, s);
         time += cfg.n_steps * cfg.tau;
       }
     STMG_CUDA(cudaStreamSynchronize(s));
+  }
+
+  // ErrorCalculator::evaluate_error (exact_solution.h:217-299): per step and
+  // QGauss(r+1) time point the FE function in time (Lagrange basis over the
+  // step's time dofs; cGP takes the previous value as its first node), then
+  // the space integrals; sums tau w_q |e|^2 (L2, H1) and the largest |e|.
+  void
+  SlabSolver::accumulate_errors(const std::vector<double> &tq, cudaStream_t s)
+  {
+    const auto      type = tfe::Type(cfg.time_type);
+    const MeshView &m    = meshes.back()->v;
+    std::vector<double> eq, ew, sx, sw;
+    tfe::gauss(cfg.time_degree + 1, eq, ew);
+    const int nq = cfg.time_degree + 1;
+    tfe::gauss(nq, sx, sw);
+    ErrTab et{};
+    et.nq = nq;
+    et.p1 = m.p + 1;
+    {
+      const FETables     &t = host_tables();
+      std::vector<double> xs(t.xs[m.p], t.xs[m.p] + m.p + 1);
+      for (int q = 0; q < nq; ++q)
+        {
+          et.gx[q] = sx[q];
+          et.gw[q] = sw[q];
+          for (int a = 0; a <= m.p; ++a)
+            {
+              et.phi[q][a] = tfe::lagrange(xs, a, sx[q]);
+              // derivative of the Lagrange polynomial: sum over the dropped factor
+              double dv = 0;
+              for (int k = 0; k <= m.p; ++k)
+                {
+                  if (k == a)
+                    continue;
+                  double term = 1.0 / (xs[a] - xs[k]);
+                  for (int l = 0; l <= m.p; ++l)
+                    if (l != a && l != k)
+                      term *= (sx[q] - xs[l]) / (xs[a] - xs[l]);
+                  dv += term;
+                }
+              et.dphi[q][a] = dv;
+            }
+        }
+    }
+    if (!err_buf.ptr)
+      {
+        err_buf.alloc(std::size_t(3) * m.ncells + 3);
+        err_num.alloc(N);
+      }
+    double *cl2 = err_buf.ptr, *ch1 = cl2 + m.ncells, *cl8 = ch1 + m.ncells, *out = cl8 + m.ncells;
+    for (int it = 0; it < cfg.n_steps; ++it)
+      for (std::size_t q = 0; q < eq.size(); ++q)
+        {
+          const double tt = time + cfg.tau * it + eq[q] * cfg.tau;
+          STMG_CUDA(cudaMemsetAsync(err_num.ptr, 0, N * 8, s));
+          const double *pu = it == 0 ? prev_x.ptr : x.ptr + (ni * it - 1) * N;
+          for (std::size_t i = 0; i < tq.size(); ++i)
+            {
+              const double b = tfe::lagrange(tq, int(i), eq[q]);
+              if (b == 0.0)
+                continue;
+              const double *src = type == tfe::DG ? x.ptr + (ni * it + i) * N : (i == 0 ? pu : x.ptr + (ni * it + i - 1) * N);
+              axpby<double>(N, b, src, 1.0, err_num.ptr, s);
+            }
+          const unsigned nbk = unsigned((m.ncells + 127) / 128);
+          if (m.dim == 2)
+            err_cell_kernel<2><<<nbk, 128, 0, s>>>(m, et, err_num.ptr, tt, cfg.frequency, cl2, ch1, cl8);
+          else
+            err_cell_kernel<3><<<nbk, 128, 0, s>>>(m, et, err_num.ptr, tt, cfg.frequency, cl2, ch1, cl8);
+          count_launch();
+          STMG_CUDA(cudaGetLastError());
+          err_reduce_kernel<<<1, 1024, 0, s>>>(m.ncells, cl2, ch1, cl8, out);
+          count_launch();
+          STMG_CUDA(cudaGetLastError());
+          double h[3];
+          STMG_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s));
+          STMG_CUDA(cudaStreamSynchronize(s));
+          err_l2sq += cfg.tau * ew[q] * h[0];
+          err_h1sq += cfg.tau * ew[q] * h[1];
+          err_l8 = std::max(err_l8, h[2]);
+        }
   }
 
   double

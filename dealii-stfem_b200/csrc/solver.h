@@ -148,11 +148,16 @@ namespace stmg
     DevBuf<double>                      x, v, prev_x, prev_v, rhs, F, Mf, fsrc;
     std::vector<double>                 node_x; // node coordinates (host), N x dim
     tfe::Mat                            lhsK_, rK_; // time matrices of K in the system and the rhs
+    // error norms against the manufactured solution over the slabs run since
+    // set_initial (rhs_mode 0): sums of squares and the maximum
+    double                              err_l2sq = 0, err_h1sq = 0, err_l8 = 0;
     std::unique_ptr<GMG>                gmgT;       // preconditioner of A^T (built on first use)
     std::vector<int>                    last_iterations;
 
   private:
     void force(double t, double *out, cudaStream_t s);
+    void accumulate_errors(const std::vector<double> &tq, cudaStream_t s);
+    DevBuf<double> err_buf, err_num;
   };
 
   std::vector<std::unique_ptr<Mesh>> build_meshes(const SolverConfig &cfg);

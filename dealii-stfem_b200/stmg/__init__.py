@@ -287,6 +287,12 @@ class Solver:
                                       _stream(stream)))
         return k.value
 
+    def errors(self):
+        """(linf, l2, h1) against the manufactured solution since set_initial."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        check(lib().stmg_solver_errors(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     def gradient(self, u_obs, n_slabs=None, checkpoint_every=0, stream=None):
         """Misfit J = 1/2 sum_s |U_s - O_s|^2 of the next n_slabs slabs and
         dJ/dlog(kappa) per fine cell by the adjoint slab sweep

@@ -188,6 +188,11 @@ STMG_API int stmg_solver_solution(stmg_solver_t solver, double *u, double *v);
 /* SolverFGMRES::solve of the slab system (time_integrators.h:174) on device
  * vectors x (initial guess in, solution out) and rhs */
 STMG_API int stmg_solver_solve(stmg_solver_t solver, double *x, const double *rhs, int *iterations, void *stream);
+/* Error norms of the slabs run since the last set_initial against the
+ * manufactured solution (rhs_mode 0; ErrorCalculator, exact_solution.h:
+ * 217-299): L-infinity over the time and space quadrature points, L2(0,T;L2)
+ * and L2(0,T;H1-seminorm), QGauss(r+1) in space and time. */
+STMG_API int stmg_solver_errors(stmg_solver_t solver, double *linf, double *l2, double *h1);
 /* Adjoint gradient (heat): runs n_slabs slabs from the current state and
  * returns the space-time misfit J = 1/2 sum_s |U_s - O_s|^2 over all slab
  * time dofs and nodes (u_obs: host, n_slabs x n_t x N, slab-major) and dJ/d

@@ -52,6 +52,11 @@ def test_gpu_iterations_match_tp01(g):
     _record(g, total)
     # within one iteration per slab of the reference
     assert abs(total - g["iterations"]) <= g["slabs"], (total, g["iterations"])
+    # error norms against the manufactured solution, as printed (6 digits)
+    linf, l2, h1 = s.errors()
+    assert linf == pytest.approx(g["linf"], rel=2e-5)
+    assert l2 == pytest.approx(g["l2"], rel=2e-5)
+    assert h1 == pytest.approx(g["h1"], rel=2e-5)
 
 
 @pytest.mark.parametrize("problem,ttype,k,steps", [("heat", "DG", 1, 1), ("heat", "CGP", 2, 1), ("wave", "DG", 1, 1),
