@@ -177,6 +177,23 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------- GPU arm
+def max_over_ranks(t, dist=None):
+    """The slowest rank's time (replicas run independently; the job takes
+    as long as its slowest replica)."""
+    if dist is None:
+        return t
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    tt = torch.tensor([t], device=dev, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_throughput(world, dofs_per_step, steps, t):
+    """Whole-job DoF/s of `world` replicas, each solving `steps` slabs."""
+    return world * dofs_per_step * steps / t
+
+
 def kernel_roofline(stmg, torch, w, kappa, hbm, only=None):
     """Finest-level FP32 operator and Vanka apply timed in isolation with CUDA
     events on the launching stream; algorithmic bytes per launch:
@@ -256,11 +273,7 @@ def run_ours(args):
         if dist:
             dist.barrier()
         launches = stmg.kernel_launches() - l0
-        t = e0.elapsed_time(e1) / 1e3
-        if dist:
-            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist)
         return t, its, launches
 
     t_setup = time.perf_counter()
@@ -271,7 +284,7 @@ def run_ours(args):
     t32, its32, launches = timed(solver, args.steps, args.warmup)
     clk = clocks.stop()
     dofs_step = w["nodes"] * w["nt"]
-    value = world * dofs_step * args.steps / t32
+    value = replica_throughput(world, dofs_step, args.steps, t32)
 
     # end to end through the C ABI with host buffers: per step the slab's
     # source goes host -> device (pinned) and the slab solution comes back
