@@ -194,7 +194,7 @@ def replica_throughput(world, dofs_per_step, steps, t):
     return world * dofs_per_step * steps / t
 
 
-def kernel_roofline(stmg, torch, w, kappa, hbm, only=None):
+def kernel_roofline(stmg, torch, w, kappa, hbm, only=None, fp64=False):
     """Finest-level FP32 operator and Vanka apply timed in isolation with CUDA
     events on the launching stream; algorithmic bytes per launch:
       operator: 2 n_t N 4 (read src, write dst) + cells 4 (coefficient)
@@ -203,13 +203,14 @@ def kernel_roofline(stmg, torch, w, kappa, hbm, only=None):
     mesh = stmg.Mesh(3, (n, n, n), 2, coeff=kappa)
     A, B, _, _, _ = stmg.time_weights(stmg.DG, 3, w["tau"], 1, stmg.HEAT)
     N, nt = w["nodes"], w["nt"]
-    x = torch.randn(nt * N, device="cuda", dtype=torch.float32)
+    x = torch.randn(nt * N, device="cuda", dtype=torch.float64 if fp64 else torch.float32)
     y = torch.empty_like(x)
     s = torch.cuda.current_stream()
     out = {}
-    op = stmg.Operator(mesh, A, B, dtype=stmg.F32) if only in (None, "st_apply") else None
+    op = stmg.Operator(mesh, A, B, dtype=stmg.F64 if fp64 else stmg.F32) if only in (None, "st_apply") else None
     vk = stmg.Vanka(mesh, A, B, compute=stmg.F32, storage=stmg.F32) if only in (None, "vanka_apply") else None
-    for name, fn, nbytes in (("st_apply", lambda: op.vmult(y, x), 2 * nt * N * 4 + w["cells"] * 4),
+    sz = 8 if fp64 else 4
+    for name, fn, nbytes in (("st_apply", lambda: op.vmult(y, x), 2 * nt * N * sz + w["cells"] * sz),
                              ("vanka_apply", lambda: vk.vmult(y, x), w["cells"] * (27 * 27 + 27) * 4 + 2 * nt * N * 4)):
         if only is not None and name != only:
             continue
@@ -353,8 +354,9 @@ def main():
     ap.add_argument("--refine", type=int, default=7, help="mesh 2^refine cells per direction (7: 128^3)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 V-cycle comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
-    ap.add_argument("--kernels-only", choices=["all", "st_apply", "vanka_apply"], default=None,
-                    help="only time the finest-level operator and/or Vanka apply in isolation (profiling)")
+    ap.add_argument("--kernels-only", choices=["all", "st_apply", "st_apply64", "vanka_apply"], default=None,
+                    help="only time the finest-level operator (FP32 or FP64) and/or Vanka apply in isolation "
+                         "(profiling)")
     args = ap.parse_args()
     if args.kernels_only:
         import torch
@@ -362,8 +364,8 @@ def main():
         w = workload(args.refine)
         kappa, _ = inputs(w)
         hbm, kind = peaks()
-        only = None if args.kernels_only == "all" else args.kernels_only
-        kr = kernel_roofline(stmg, torch, w, kappa, hbm, only)
+        only = None if args.kernels_only == "all" else args.kernels_only.replace("64", "")
+        kr = kernel_roofline(stmg, torch, w, kappa, hbm, only, fp64=args.kernels_only == "st_apply64")
         print(json.dumps(dict(workload=w["name"], peak_gbs=hbm, peak_kind=kind, kernels=kr)), flush=True)
         return 0
     if args.impl == "reference":
