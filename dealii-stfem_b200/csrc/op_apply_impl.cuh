@@ -289,7 +289,7 @@ namespace stmg
       const int nti = tm.nt_in, nto = tm.nt_out;
       const int ntp = NTPC == 4 ? (nti + 3) / 4 * 4 : NTPC;
       T        *bricks[2] = {reinterpret_cast<T *>(smem_raw), reinterpret_cast<T *>(smem_raw) + S::NB * ntp};
-      T        *cellbuf   = bricks[1] + S::NB * ntp; // [nto][TC][ND]
+      T        *cellbuf   = bricks[1] + S::NB * ntp; // [TC][nto][ND]
       const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
       // brick load lanes: (node along x, time value)
       const int npl = 32 / ntp, lnode = lane / ntp, li = lane - lnode * ntp;
@@ -345,7 +345,10 @@ namespace stmg
           const T *brick = bricks[buf];
           for (int w = threadIdx.x; w < nto * S::TC; w += blockDim.x)
             {
-              const int j = w / S::TC, lc = w - j * S::TC;
+              // consecutive threads take the time dofs of one cell: they
+              // share the cell's brick reads (broadcast) and write
+              // consecutive per-cell results
+              const int lc = w / nto, j = w - lc * nto;
               const int lx = lc % TX, ly = (lc / TX) % TY, lz = lc / (TX * TY);
               if (lx >= tc[0] || ly >= tc[1] || lz >= tc[2])
                 continue;
@@ -413,7 +416,7 @@ namespace stmg
                 box_apply<DIM, P>(m, qt, cell, a, b, out);
               else
                 general_apply<DIM, P>(m, qt, cx, cy, cz, cell, a, b, out);
-              T *cb = cellbuf + (j * S::TC + lc) * ND;
+              T *cb = cellbuf + (lc * nto + j) * ND;
 #pragma unroll
               for (int q = 0; q < ND; ++q)
                 cb[q] = out[q];
@@ -433,8 +436,8 @@ namespace stmg
               const bool face = bx % P == 0 && bx > 0;
               const int  cx0  = face ? bx / P - 1 : bx / P;
               const int  ax0  = face ? P : bx % P;
-              lx_base[h]      = cx0 * ND + ax0;
-              lx_dx[h]        = ND - ax0;
+              lx_base[h]      = cx0 * nto * ND + ax0;
+              lx_dx[h]        = nto * ND - ax0;
               lx_two[h]       = face && bx / P < tc[0];
               lx_in[h]        = bx > 0 && bx < e[0] - 1;
             }
@@ -446,7 +449,7 @@ namespace stmg
               const bool fy = by % P == 0 && by > 0;
               const int  cy0 = fy ? by / P - 1 : by / P, ay0 = fy ? P : by % P;
               const bool ty  = fy && by / P < tc[1];
-              const int  dy  = TX * ND - P1 * ay0;
+              const int  dy  = TX * nto * ND - P1 * ay0;
               int        cz0 = 0, az0 = 0, dz = 0;
               bool       tz  = false;
               if (DIM == 3)
@@ -455,9 +458,9 @@ namespace stmg
                   cz0           = fz ? bz / P - 1 : bz / P;
                   az0           = fz ? P : bz % P;
                   tz            = fz && bz / P < tc[2];
-                  dz            = TX * TY * ND - P1 * P1 * az0;
+                  dz            = TX * TY * nto * ND - P1 * P1 * az0;
                 }
-              const T   *cbr = cellbuf + TX * (cy0 + TY * cz0) * ND + P1 * (ay0 + P1 * az0);
+              const T   *cbr = cellbuf + TX * (cy0 + TY * cz0) * nto * ND + P1 * (ay0 + P1 * az0);
               const long long grow = c0[0] * P + (long long)m.nn[0] * ((c0[1] * P + by) + (long long)m.nn[1] * (c0[2] * P + bz));
               const bool yzin = by > 0 && by < e[1] - 1 && (DIM < 3 || (bz > 0 && bz < e[2] - 1));
               // shell slot of this row: x faces by (y, z); y and z faces by x
@@ -489,7 +492,7 @@ namespace stmg
                   const T   *cj    = c;
                   long long  gj    = grow + bx; // index into dst and rhs
                   T         *sj    = shell + (long long)tile * nto * tl.tile_stride + slot;
-                  for (int j = 0; j < nto; ++j, cj += S::TC * ND, gj += m.N, sj += tl.tile_stride)
+                  for (int j = 0; j < nto; ++j, cj += ND, gj += m.N, sj += tl.tile_stride)
                     {
                       T s = cj[0];
                       if (two)
