@@ -80,6 +80,67 @@ namespace stmg
         }
     }
 
+    // K a + M b on a cartesian cell with two live arrays: one pass per
+    // direction over the 1-D pencils, each pencil updated in place,
+    //   z: a <- Mz a,  b <- Mz b + Kz a
+    //   y: a <- My a,  b <- My b + Ky a
+    //   x:             b <- Mx b + Kx a
+    // (= Kx My Mz a + Mx Ky Mz a + Mx My Kz a + Mx My Mz b); result in b.
+    template <int DIM, int P, typename T>
+    __device__ __forceinline__ void
+    cart_apply_pencils(const Cart1D<T> &c, T *a, T *b)
+    {
+      constexpr int P1 = P + 1;
+      auto pass = [&](int d, int base, int stride, bool keep_a) {
+        T va[P1], vb[P1];
+#pragma unroll
+        for (int k = 0; k < P1; ++k)
+          {
+            va[k] = a[base + k * stride];
+            vb[k] = b[base + k * stride];
+          }
+#pragma unroll
+        for (int i = 0; i < P1; ++i)
+          {
+            T ma = T(0), sb = T(0);
+#pragma unroll
+            for (int k = 0; k < P1; ++k)
+              {
+                const T mik = c.M[d][i * P1 + k];
+                if (keep_a)
+                  ma += mik * va[k];
+                sb += mik * vb[k] + c.K[d][i * P1 + k] * va[k];
+              }
+            if (keep_a)
+              a[base + i * stride] = ma;
+            b[base + i * stride] = sb;
+          }
+      };
+      if constexpr (DIM == 3)
+        {
+#pragma unroll
+          for (int o = 0; o < P1 * P1; ++o)
+            pass(2, o, P1 * P1, true);
+#pragma unroll
+          for (int z = 0; z < P1; ++z)
+#pragma unroll
+            for (int x = 0; x < P1; ++x)
+              pass(1, x + z * P1 * P1, P1, true);
+#pragma unroll
+          for (int r = 0; r < P1 * P1; ++r)
+            pass(0, r * P1, 1, false);
+        }
+      else
+        {
+#pragma unroll
+          for (int x = 0; x < P1; ++x)
+            pass(1, x, P1, true);
+#pragma unroll
+          for (int y = 0; y < P1; ++y)
+            pass(0, y * P1, 1, false);
+        }
+    }
+
     // K a + M b on a Q1-mapped cell with QGauss(p+1) and a coefficient per
     // cell or per quadrature point.
     template <int DIM, int P, typename T>
@@ -276,7 +337,7 @@ namespace stmg
     //     mesh).
     // NTPC: 1 or 2 time values per node, or 4 for multiples of four.
     template <int DIM, int P, typename T, int MODE, int TX, int TY, int TZ, int NTPC>
-    __global__ void __launch_bounds__(256, (sizeof(T) == 4 && MODE != 0) ? 2 : 1)
+    __global__ void __launch_bounds__(256, (MODE == 1 || (sizeof(T) == 4 && MODE == 2)) ? 2 : 1)
     st_apply_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<T> tm,
                     const __grid_constant__ Cart1D<T> c1, const __grid_constant__ QTab<T> qt,
                     const T *__restrict__ src, T *__restrict__ dst, T *__restrict__ shell, const OutMode<T> om)
@@ -409,17 +470,28 @@ namespace stmg
                         }
                     }
                 }
-              T out[ND];
-              if constexpr (MODE == 1)
-                cart_apply<DIM, P>(c1, a, b, out);
-              else if constexpr (MODE == 2)
-                box_apply<DIM, P>(m, qt, cell, a, b, out);
-              else
-                general_apply<DIM, P>(m, qt, cx, cy, cz, cell, a, b, out);
               T *cb = cellbuf + (lc * nto + j) * ND;
+              if constexpr (MODE == 1 && sizeof(T) == 8)
+                {
+                  // FP64: two live arrays keep the kernel at two CTAs per SM
+                  cart_apply_pencils<DIM, P>(c1, a, b); // result in b
 #pragma unroll
-              for (int q = 0; q < ND; ++q)
-                cb[q] = out[q];
+                  for (int q = 0; q < ND; ++q)
+                    cb[q] = b[q];
+                }
+              else
+                {
+                  T out[ND];
+                  if constexpr (MODE == 1)
+                    cart_apply<DIM, P>(c1, a, b, out);
+                  else if constexpr (MODE == 2)
+                    box_apply<DIM, P>(m, qt, cell, a, b, out);
+                  else
+                    general_apply<DIM, P>(m, qt, cx, cy, cz, cell, a, b, out);
+#pragma unroll
+                  for (int q = 0; q < ND; ++q)
+                    cb[q] = out[q];
+                }
             }
           __syncthreads();
 
