@@ -15,6 +15,8 @@
 // the cells with the operator's tile / brick / shell scheme.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <complex>
 #include <cstring>
 
 #include <cuda_bf16.h>
@@ -493,6 +495,260 @@ namespace stmg
 
   } // namespace
 
+  namespace
+  {
+    using cplx = std::complex<double>;
+
+    // x = M^{-1} y for a small complex matrix (Gaussian elimination with
+    // partial pivoting); false if singular
+    bool
+    csolve(int n, std::vector<cplx> M, std::vector<cplx> &x)
+    {
+      for (int k = 0; k < n; ++k)
+        {
+          int piv = k;
+          for (int i = k + 1; i < n; ++i)
+            if (std::abs(M[i * n + k]) > std::abs(M[piv * n + k]))
+              piv = i;
+          if (std::abs(M[piv * n + k]) < 1e-300)
+            return false;
+          if (piv != k)
+            {
+              for (int j = 0; j < n; ++j)
+                std::swap(M[k * n + j], M[piv * n + j]);
+              std::swap(x[k], x[piv]);
+            }
+          for (int i = k + 1; i < n; ++i)
+            {
+              const cplx f = M[i * n + k] / M[k * n + k];
+              for (int j = k; j < n; ++j)
+                M[i * n + j] -= f * M[k * n + j];
+              x[i] -= f * x[k];
+            }
+        }
+      for (int i = n - 1; i >= 0; --i)
+        {
+          cplx s = x[i];
+          for (int j = i + 1; j < n; ++j)
+            s -= M[i * n + j] * x[j];
+          x[i] = s / M[i * n + i];
+        }
+      return true;
+    }
+
+    // Real eigen-decomposition of C = Beta^{-1} Alpha for n <= 4: the
+    // characteristic polynomial (Faddeev-LeVerrier), its roots by
+    // Durand-Kerner iteration polished by Newton, eigenvectors by inverse
+    // iteration on the shifted matrix; accepted when C S = S Lambda holds to
+    // 1e-10 and S is well conditioned.
+    TimeEig
+    time_eigen(int n, const double *A, const double *B)
+    {
+      TimeEig te{};
+      te.nt = n;
+      if (n < 1 || n > 4)
+        return te;
+      // C = B^{-1} A
+      std::vector<cplx> Bc(n * n), C(n * n);
+      for (int i = 0; i < n * n; ++i)
+        Bc[i] = B[i];
+      for (int j = 0; j < n; ++j)
+        {
+          std::vector<cplx> col(n);
+          for (int i = 0; i < n; ++i)
+            col[i] = A[i * n + j];
+          if (!csolve(n, Bc, col))
+            return te;
+          for (int i = 0; i < n; ++i)
+            C[i * n + j] = col[i];
+        }
+      // characteristic polynomial p(x) = x^n + c[1] x^{n-1} + ... + c[n]
+      std::vector<double> c(n + 1, 0.0);
+      c[0] = 1;
+      std::vector<double> Mk(n * n, 0.0), AM(n * n);
+      for (int k = 1; k <= n; ++k)
+        {
+          // M_k = C M_{k-1} + c_{k-1} I, c_k = -tr(C M_k) / k
+          std::vector<double> Mn(n * n, 0.0);
+          for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+              {
+                double s = 0;
+                for (int l = 0; l < n; ++l)
+                  s += C[i * n + l].real() * Mk[l * n + j];
+                Mn[i * n + j] = s + (i == j ? c[k - 1] : 0.0);
+              }
+          double tr = 0;
+          for (int i = 0; i < n; ++i)
+            for (int l = 0; l < n; ++l)
+              tr += C[i * n + l].real() * Mn[l * n + i];
+          c[k] = -tr / k;
+          Mk   = Mn;
+        }
+      auto peval = [&](cplx x) {
+        cplx v = 1;
+        for (int k = 1; k <= n; ++k)
+          v = v * x + c[k];
+        return v;
+      };
+      auto pder = [&](cplx x) {
+        cplx v = double(n);
+        for (int k = 1; k < n; ++k)
+          v = v * x + double(n - k) * c[k];
+        return v;
+      };
+      double rad = 0;
+      for (int k = 1; k <= n; ++k)
+        rad = std::max(rad, std::abs(c[k]));
+      rad = 1 + rad;
+      std::vector<cplx> r(n);
+      for (int k = 0; k < n; ++k)
+        r[k] = std::polar(rad * 0.9, 0.4 + 2 * 3.14159265358979323846 * k / n);
+      for (int it = 0; it < 500; ++it)
+        {
+          double moved = 0;
+          for (int k = 0; k < n; ++k)
+            {
+              cplx den = 1;
+              for (int j = 0; j < n; ++j)
+                if (j != k)
+                  den *= r[k] - r[j];
+              const cplx d = peval(r[k]) / den;
+              r[k] -= d;
+              moved = std::max(moved, std::abs(d));
+            }
+          if (moved < 1e-15 * rad)
+            break;
+        }
+      for (int k = 0; k < n; ++k)
+        for (int it = 0; it < 3; ++it)
+          {
+            const cplx dp = pder(r[k]);
+            if (std::abs(dp) > 0)
+              r[k] -= peval(r[k]) / dp;
+          }
+      // order: real roots, then complex pairs (positive imaginary part first)
+      std::vector<cplx> lam;
+      for (int k = 0; k < n; ++k)
+        if (std::abs(r[k].imag()) <= 1e-10 * (1 + std::abs(r[k])))
+          lam.push_back(cplx(r[k].real(), 0.0));
+      for (int k = 0; k < n; ++k)
+        if (r[k].imag() > 1e-10 * (1 + std::abs(r[k])))
+          {
+            lam.push_back(r[k]);
+            lam.push_back(std::conj(r[k]));
+          }
+      if (int(lam.size()) != n)
+        return te;
+      // distinct eigenvalues only
+      for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j)
+          if (std::abs(lam[i] - lam[j]) < 1e-8 * (1 + std::abs(lam[i])))
+            return te;
+      // eigenvectors by inverse iteration; real matrix Sr in the real block form
+      std::vector<double> Sr(n * n, 0.0);
+      for (int k = 0; k < n; ++k)
+        {
+          const bool pair = lam[k].imag() > 0;
+          if (lam[k].imag() < 0)
+            continue; // filled with its partner
+          const cplx sh = lam[k] + cplx(1e-9 * (1 + std::abs(lam[k])), 1e-9 * (1 + std::abs(lam[k])));
+          std::vector<cplx> M(n * n), v(n, cplx(1.0, 0.5));
+          for (int i = 0; i < n * n; ++i)
+            M[i] = C[i] - (i / n == i % n ? sh : cplx(0));
+          for (int it = 0; it < 3; ++it)
+            {
+              if (!csolve(n, M, v))
+                return te;
+              double nv = 0;
+              for (auto &e : v)
+                nv = std::max(nv, std::abs(e));
+              for (auto &e : v)
+                e /= nv;
+            }
+          for (int i = 0; i < n; ++i)
+            {
+              Sr[i * n + k] = v[i].real();
+              if (pair)
+                Sr[i * n + k + 1] = v[i].imag();
+            }
+          te.kind[k] = pair ? 2 : 1;
+          te.a[k]    = float(lam[k].real());
+          te.b[k]    = float(lam[k].imag());
+          if (pair)
+            {
+              te.kind[k + 1] = 3;
+              te.a[k + 1]    = te.a[k];
+              te.b[k + 1]    = te.b[k];
+            }
+        }
+      // residual of C Sr = Sr Lambda_r
+      double res = 0, cn = 0;
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < n; ++k)
+          {
+            double cs = 0;
+            for (int l = 0; l < n; ++l)
+              cs += C[i * n + l].real() * Sr[l * n + k];
+            double sl;
+            if (te.kind[k] == 1)
+              sl = Sr[i * n + k] * lam[k].real();
+            else if (te.kind[k] == 2)
+              sl = lam[k].real() * Sr[i * n + k] - lam[k].imag() * Sr[i * n + k + 1];
+            else // second column of a pair: lam[k - 1] carries the positive imaginary part
+              sl = lam[k - 1].imag() * Sr[i * n + k - 1] + lam[k - 1].real() * Sr[i * n + k];
+            res = std::max(res, std::abs(cs - sl));
+            cn  = std::max(cn, std::abs(C[i * n + k]));
+          }
+      if (res > 1e-10 * (1 + cn))
+        return te;
+      // G = Sr^{-1} B^{-1}; condition estimate from |Sr| |Sr^{-1}|
+      std::vector<cplx> Src(n * n);
+      for (int i = 0; i < n * n; ++i)
+        Src[i] = Sr[i];
+      double ninv = 0, ns = 0;
+      std::vector<double> Sinv(n * n);
+      for (int j = 0; j < n; ++j)
+        {
+          std::vector<cplx> e(n, 0.0);
+          e[j] = 1;
+          if (!csolve(n, Src, e))
+            return te;
+          for (int i = 0; i < n; ++i)
+            Sinv[i * n + j] = e[i].real();
+        }
+      for (int i = 0; i < n * n; ++i)
+        {
+          ninv = std::max(ninv, std::abs(Sinv[i]));
+          ns   = std::max(ns, std::abs(Sr[i]));
+        }
+      if (ns * ninv * n > 1e5)
+        return te;
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+          {
+            // G = Sinv B^{-1}: solve B^T g_row = Sinv_row
+            te.S[i * n + j] = float(Sr[i * n + j]);
+          }
+      std::vector<cplx> BT(n * n);
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+          BT[i * n + j] = B[j * n + i];
+      for (int i = 0; i < n; ++i)
+        {
+          std::vector<cplx> row(n);
+          for (int j = 0; j < n; ++j)
+            row[j] = Sinv[i * n + j];
+          if (!csolve(n, BT, row))
+            return te;
+          for (int j = 0; j < n; ++j)
+            te.G[i * n + j] = float(row[j].real());
+        }
+      te.use = 1;
+      return te;
+    }
+  } // namespace
+
   Vanka::Vanka(Mesh *mesh_, int nt_, const double *A, const double *B, int compute_, int storage_)
     : mesh(mesh_)
     , nt(nt_)
@@ -515,6 +771,12 @@ namespace stmg
         tm32.A[i] = float(A[i]);
         tm32.B[i] = float(B[i]);
       }
+    {
+      const char *e = std::getenv("STMG_VANKA_EIG");
+      if (!(e && e[0] == '0'))
+        teig = time_eigen(nt, A, B);
+      teig.nt = nt;
+    }
     const std::size_t nd   = mesh->nd;
     const std::size_t elem = storage == STMG_F64 ? 8 : (storage == STMG_F32 ? 4 : 2);
     auto              pad  = [](std::size_t b) { return (b + 15) / 16 * 16; };

@@ -6,6 +6,20 @@
 
 namespace stmg
 {
+  // The n_t x n_t mode systems (mu Alpha + Beta) z = y of the streamed
+  // apply in the eigenbasis of C = Beta^{-1} Alpha = S Lambda S^{-1} (real
+  // form: 1x1 blocks for real eigenvalues, 2x2 blocks [[a, b], [-b, a]] for
+  // complex pairs a +- ib): z = S (mu Lambda + I)^{-1} G y, G = S^{-1} Beta^{-1}.
+  // use = 0 keeps the pivoted elimination (decomposition failed or too
+  // ill-conditioned). Kernel parameter.
+  struct TimeEig
+  {
+    int   use, nt;
+    int   kind[MAX_NT]; // 1: real eigenvalue, 2: first of a complex pair, 3: second of a pair
+    float a[MAX_NT], b[MAX_NT];
+    float G[16], S[16]; // n_t x n_t row-major (n_t <= 4)
+  };
+
   class Vanka
   {
   public:
@@ -46,6 +60,7 @@ namespace stmg
     DevBuf<unsigned char> shell; // tile face slots (scratch)
     TimeMats<double>      tm64;
     TimeMats<float>       tm32;
+    TimeEig               teig{};
   };
 
   // apply of one (dimension, degree), defined in vanka_apply_d<D>p<P>.cu

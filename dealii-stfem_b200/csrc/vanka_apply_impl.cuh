@@ -302,6 +302,48 @@ namespace stmg
         }
     }
 
+    // (mu A + B) z = y through the eigenbasis of B^{-1} A (see TimeEig):
+    // w = G y, then per real eigenvalue w_k /= mu a_k + 1 and per complex pair
+    // the 2x2 block [[mu a + 1, mu b], [-mu b, mu a + 1]] inverted, z = S w.
+    template <int NT>
+    __device__ __forceinline__ void
+    mode_solve_eig(const TimeEig &te, float mu, const float (&y)[NT], float (&z)[NT])
+    {
+      float w[NT];
+#pragma unroll
+      for (int i = 0; i < NT; ++i)
+        {
+          float s = 0.0f;
+#pragma unroll
+          for (int j = 0; j < NT; ++j)
+            s = fmaf(te.G[i * NT + j], y[j], s);
+          w[i] = s;
+        }
+#pragma unroll
+      for (int k = 0; k < NT; ++k)
+        {
+          const float d = fmaf(mu, te.a[k], 1.0f);
+          if (te.kind[k] == 1)
+            w[k] *= __frcp_rn(d);
+          else if (te.kind[k] == 2 && k + 1 < NT)
+            {
+              const float e = mu * te.b[k], inv = __frcp_rn(fmaf(d, d, e * e));
+              const float u = w[k], v = w[k + 1];
+              w[k]          = inv * fmaf(d, u, -e * v);
+              w[k + 1]      = inv * fmaf(e, u, d * v);
+            }
+        }
+#pragma unroll
+      for (int i = 0; i < NT; ++i)
+        {
+          float s = 0.0f;
+#pragma unroll
+          for (int j = 0; j < NT; ++j)
+            s = fmaf(te.S[i * NT + j], w[j], s);
+          z[i] = s;
+        }
+    }
+
     // NT time values of one node, stored contiguously (NTP = padded count)
     template <int NT>
     struct TimeVec
@@ -377,9 +419,9 @@ namespace stmg
     template <int DIM, int P, typename TS, int NT, int TX, int TY, int TZ>
     __global__ void __launch_bounds__(256, 2)
     vanka_stream_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<float> tm,
-                        const unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int cpc,
-                        const float *__restrict__ src, float *__restrict__ dst, float *__restrict__ shell,
-                        const OutMode<float> om)
+                        const __grid_constant__ TimeEig te, const unsigned char *__restrict__ rec, int rec_bytes,
+                        int mu_off, int cpc, const float *__restrict__ src, float *__restrict__ dst,
+                        float *__restrict__ shell, const OutMode<float> om)
     {
       using S           = TileShape<DIM, P, TX, TY, TZ>;
       using TV          = TimeVec<NT>;
@@ -539,7 +581,10 @@ namespace stmg
                         }
                     }
                   float z[NT];
-                  mode_solve_reg<NT>(tm, mu[mm], y, z);
+                  if (te.use)
+                    mode_solve_eig<NT>(te, mu[mm], y, z);
+                  else
+                    mode_solve_reg<NT>(tm, mu[mm], y, z);
                   TV::store(zb + mm * NTP, z);
                 }
               __syncwarp();
@@ -662,8 +707,8 @@ namespace stmg
       const std::size_t smem = vk.smem_bytes(vk.shape);
       auto              kern = vanka_stream_kernel<DIM, P, TS, NT, Sh::TX, Sh::TY, Sh::TZ>;
       const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, tl.n_tiles);
-      kern<<<grid, 256, smem, s>>>(m, tl, vk.tmats<float>(), vk.V.ptr, vk.rec_bytes, vk.mu_off, vk.colour_cells,
-                                   src, dst, reinterpret_cast<float *>(vk.shell.ptr), om);
+      kern<<<grid, 256, smem, s>>>(m, tl, vk.tmats<float>(), vk.teig, vk.V.ptr, vk.rec_bytes, vk.mu_off,
+                                   vk.colour_cells, src, dst, reinterpret_cast<float *>(vk.shell.ptr), om);
       count_launch();
       STMG_CUDA(cudaGetLastError());
       if (tl.n_tiles > 1)
