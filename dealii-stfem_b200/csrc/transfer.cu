@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "async_copy.cuh"
 #include "kernels_common.cuh"
 #include "transfer.h"
 
@@ -78,8 +79,13 @@ namespace stmg
               const int g[3] = {q0[0] + x, q0[1] + y, DIM == 3 ? q0[2] + z : 0};
               bool      ok   = g[0] < cm.nn[0] && g[1] < cm.nn[1] && (DIM < 3 || g[2] < cm.nn[2]);
               ok             = ok && !is_boundary_node(cm, g[0], g[1], g[2]);
-              sc[i] = ok ? src[j * cm.N + g[0] + (long long)cm.nn[0] * (g[1] + (long long)cm.nn[1] * g[2])] : T(0);
+              cp_async_small<sizeof(T)>(sc + i,
+                                        ok ? src + j * cm.N + g[0] + (long long)cm.nn[0] * (g[1] + (long long)cm.nn[1] * g[2])
+                                           : src,
+                                        ok);
             }
+          cp_async_commit();
+          cp_async_wait<0>();
           __syncthreads();
           // x: sc[z][y][cx] -> s1[z][y][fx]
           for (int i = threadIdx.x; i < NZC * LC * LF; i += blockDim.x)
@@ -187,9 +193,15 @@ namespace stmg
               bool      ok   = g[0] >= 0 && g[1] >= 0 && g[0] < fm.nn[0] && g[1] < fm.nn[1];
               if (DIM == 3)
                 ok = ok && g[2] >= 0 && g[2] < fm.nn[2];
-              ok    = ok && !is_boundary_node(fm, g[0], g[1], g[2]);
-              sf[i] = ok ? src[j * fm.N + g[0] + (long long)fm.nn[0] * (g[1] + (long long)fm.nn[1] * g[2])] : T(0);
+              ok = ok && !is_boundary_node(fm, g[0], g[1], g[2]);
+              // asynchronous copy (zero fill outside): all loads of the block in flight at once
+              cp_async_small<sizeof(T)>(sf + i,
+                                        ok ? src + j * fm.N + g[0] + (long long)fm.nn[0] * (g[1] + (long long)fm.nn[1] * g[2])
+                                           : src,
+                                        ok);
             }
+          cp_async_commit();
+          cp_async_wait<0>();
           __syncthreads();
           for (int i = threadIdx.x; i < NZR * LR * LQ; i += blockDim.x)
             {
