@@ -250,12 +250,15 @@ namespace oracle
           x[i] += w * z[i];
       }
 
+      // MGSmootherPrecondition(steps = 1, variable) (gmg.h:726-730): 2^(L-1-l)
+      // smoother steps on level l, each PreconditionRelaxation step running
+      // n_iterations = smoothing_steps relaxations (gmg.h:721)
       unsigned
       steps(std::size_t l) const
       {
-        unsigned s = cfg.smoothing_steps;
+        unsigned s = 1;
         if (cfg.variable)
-          s *= 1u << (h.levels.size() - 1 - l);
+          s <<= h.levels.size() - 1 - l;
         return s;
       }
 

@@ -167,3 +167,22 @@ def test_gpu_wave_bf16_vanka_keeps_iterations():
     its16, u16 = out[stmg.BF16]
     assert np.all(np.abs(its16 - its32) <= 1), (its16, its32)
     assert np.linalg.norm(u16 - u32) <= 1e-7 * np.linalg.norm(u32)
+
+
+def test_gpu_c1_plain_fp64_matches_oracle():
+    """The plain FP64 configuration: 2-D unit square, 16^2 Q2 cells, dG(1),
+    dt = 1/64, 64 slabs, manufactured u = sin(pi x) sin(pi y) sin(pi t)
+    (frequency 1/2), 2 pre/post sweeps, all-FP64 multigrid, 1e-10 relative
+    residual. GPU and oracle: iterations per slab within one, error norms to
+    1e-6."""
+    import stmg
+    kw = dict(dim=2, refine=4, n_steps=1, tau=1 / 64, fe_degree_min=0, n_steps_min=1, tol=1e-10, abs_tol=1e-14,
+              frequency=0.5, smoothing_steps=2)
+    ref = orc.run(p=2, r=1, ttype=orc.DG, problem=orc.HEAT, n_slabs=64, mg_float=False, compute_errors=True, **kw)
+    s = stmg.Solver(degree=2, time_degree=1, time_type=stmg.DG, problem=stmg.HEAT, mg_dtype=stmg.F64, **kw)
+    its = s.run(64)
+    assert np.all(np.abs(its - ref["iterations"]) <= 1), (its, ref["iterations"])
+    linf, l2, h1 = s.errors()
+    assert linf == pytest.approx(ref["linf"], rel=1e-6)
+    assert l2 == pytest.approx(ref["l2"], rel=1e-6)
+    assert h1 == pytest.approx(ref["h1"], rel=1e-6)
