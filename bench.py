@@ -362,6 +362,56 @@ def run_ours(args):
     return 0
 
 
+def run_adjoint(args):
+    """--adjoint: the adjoint-gradient configuration: heat, 32^3 Q2 cells,
+    dG(1), 16 slabs of dt = 1/16, per-cell log-coefficient ~ N(0, 1),
+    observations from a forward FP64 solve with a perturbed field plus 1e-3
+    relative noise; the misfit gradient with checkpoints every 4 slabs
+    (FP64 multigrid, 1e-12), timed, and checked against central finite
+    differences on --fd random unit directions (h = 1e-4)."""
+    import torch
+    import stmg
+    n, S = 32, 16
+    rng = np.random.default_rng(SEED)
+    theta = rng.normal(0.0, 1.0, n ** 3)
+    f = np.ones((2 * n + 1) ** 3)
+    kw = dict(dim=3, refine=5, degree=2, time_degree=1, time_type=stmg.DG, problem=stmg.HEAT, n_steps=1, tau=1 / 16,
+              fe_degree_min=0, n_steps_min=1, rhs_mode=1, f_nodal=f, tol=1e-12, abs_tol=1e-300, mg_dtype=stmg.F64)
+
+    def solver(th):
+        return stmg.Solver(fine_coeff=np.exp(th), **kw)
+
+    def forward(th):
+        sv, out = solver(th), []
+        for _ in range(S):
+            sv.run(1)
+            u, _ = sv.solution(want_v=False)
+            out.append(u)
+        return np.array(out)
+
+    clean = forward(0.9 * theta)
+    obs = clean * (1 + 1e-3 * rng.standard_normal(clean.shape))
+    s = solver(theta)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, g, itf, ita = s.gradient(obs, checkpoint_every=4)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    checks = []
+    for _ in range(args.fd):
+        d = rng.standard_normal(theta.size)
+        d /= np.linalg.norm(d)
+        h = 1e-4
+        Jp = 0.5 * float(np.sum((forward(theta + h * d) - obs) ** 2))
+        Jm = 0.5 * float(np.sum((forward(theta - h * d) - obs) ** 2))
+        fd = (Jp - Jm) / (2 * h)
+        checks.append(dict(gd=float(g @ d), fd=fd, rel=abs(float(g @ d) - fd) / max(abs(fd), 1e-300)))
+    print(json.dumps(dict(workload="heat3d-32^3-Q2-dG1-16slabs-adjoint", misfit=J, gradient_seconds=t,
+                          fgmres_forward=int(itf.sum()), fgmres_adjoint=int(ita.sum()), checkpoint_every=4,
+                          fd_checks=checks)), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -374,7 +424,11 @@ def main():
     ap.add_argument("--kernels-only", choices=["all", "st_apply", "st_apply64", "vanka_apply"], default=None,
                     help="only time the finest-level operator (FP32 or FP64) and/or Vanka apply in isolation "
                          "(profiling)")
+    ap.add_argument("--adjoint", action="store_true", help="time the adjoint gradient configuration")
+    ap.add_argument("--fd", type=int, default=2, help="finite-difference directions checked with --adjoint")
     args = ap.parse_args()
+    if args.adjoint:
+        return run_adjoint(args)
     if args.kernels_only:
         import torch
         import stmg
