@@ -362,6 +362,74 @@ def run_ours(args):
     return 0
 
 
+def run_config(args):
+    """--config c1|c2|c3: the other configurations of the slab solve, timed
+    the same way as the main line (device events, inputs resident, W warm-up
+    slabs then K timed slabs) and compared across multigrid precisions:
+      c1  2-D 16^2 Q2, dG(1), dt 1/64, frequency 1/2, 2 sweeps, FP64, tol 1e-10;
+      c2  3-D 32^3 Q3, vertices moved +-0.2h, kappa = 10^U(-2,2), dG(2),
+          dt 1/32, f = 1: FP32 vs FP64 multigrid;
+      c3  3-D wave 64^3 Q2, c^2 in {0.5, 1, 4}, dG(2), dt 1/128, Gaussian
+          pulse, v0 = 0, f = 0: Vanka stored in FP32 vs BF16."""
+    import torch
+    import meshes
+    import stmg
+    rng = np.random.default_rng(SEED)
+    init = None
+    if args.config == "c1":
+        name = "heat2d-16^2-Q2-dG1-c1"
+        base = dict(dim=2, refine=4, degree=2, time_degree=1, time_type=stmg.DG, problem=stmg.HEAT, n_steps=1,
+                    tau=1 / 64, fe_degree_min=0, n_steps_min=1, tol=1e-10, abs_tol=1e-14, frequency=0.5,
+                    smoothing_steps=2)
+        variants = {"fp64-mg": dict(mg_dtype=stmg.F64)}
+    elif args.config == "c2":
+        n = 32
+        name = "heat3d-32^3-Q3-dG2-distorted-c2"
+        V = meshes.vertices(3, (n, n, n), distort=0.2, seed=SEED)
+        kappa = 10.0 ** rng.uniform(-2, 2, n ** 3)
+        base = dict(dim=3, refine=5, degree=3, time_degree=2, time_type=stmg.DG, problem=stmg.HEAT, n_steps=1,
+                    tau=1 / 32, fe_degree_min=0, n_steps_min=1, tol=1e-8, abs_tol=1e-300, rhs_mode=1,
+                    f_nodal=np.ones((3 * n + 1) ** 3), fine_coeff=kappa, fine_vertices=V)
+        variants = {"fp32-mg": dict(mg_dtype=stmg.F32), "fp64-mg": dict(mg_dtype=stmg.F64)}
+    else:
+        n = 64
+        name = "wave3d-64^3-Q2-dG2-c3"
+        c2 = rng.choice([0.5, 1.0, 4.0], size=n ** 3)
+        X = meshes.vertices(3, (2 * n, 2 * n, 2 * n))
+        u0 = np.exp(-np.sum((X - 0.5) ** 2, axis=1) / 0.01)
+        u0[meshes.boundary_mask(3, (n, n, n), 2)] = 0.0
+        init = (u0, np.zeros_like(u0))
+        base = dict(dim=3, refine=6, degree=2, time_degree=2, time_type=stmg.DG, problem=stmg.WAVE, n_steps=1,
+                    tau=1 / 128, fe_degree_min=0, n_steps_min=1, tol=1e-8, abs_tol=1e-300, rhs_mode=2,
+                    fine_coeff=c2)
+        variants = {"fp32-vanka": dict(mg_dtype=stmg.F32, vanka_storage=stmg.F32),
+                    "bf16-vanka": dict(mg_dtype=stmg.F32, vanka_storage=stmg.BF16)}
+    out = {}
+    for vname, vkw in variants.items():
+        s = stmg.Solver(**base, **vkw)
+        if init is not None:
+            s.set_initial(*init)
+        s.run(args.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        its = s.run(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        dofs = s.n_nodes * s.n_blocks * args.steps
+        entry = dict(value=dofs / t, unit="DoF/s", ms_per_step=1e3 * t / args.steps,
+                     fgmres_iterations=[int(i) for i in its])
+        if args.config == "c1":
+            entry["errors"] = dict(zip(("linf", "l2", "h1"), s.errors()))
+        out[vname] = entry
+        del s
+        torch.cuda.empty_cache()
+    print(json.dumps(dict(workload=name, steps=args.steps, warmup=args.warmup, slabs=args.warmup + args.steps,
+                          variants=out)), flush=True)
+    return 0
+
+
 def run_adjoint(args):
     """--adjoint: the adjoint-gradient configuration: heat, 32^3 Q2 cells,
     dG(1), 16 slabs of dt = 1/16, per-cell log-coefficient ~ N(0, 1),
@@ -425,10 +493,14 @@ def main():
                     help="only time the finest-level operator (FP32 or FP64) and/or Vanka apply in isolation "
                          "(profiling)")
     ap.add_argument("--adjoint", action="store_true", help="time the adjoint gradient configuration")
+    ap.add_argument("--config", choices=["c1", "c2", "c3"], default=None,
+                    help="time one of the other configurations (not the main metric line)")
     ap.add_argument("--fd", type=int, default=2, help="finite-difference directions checked with --adjoint")
     args = ap.parse_args()
     if args.adjoint:
         return run_adjoint(args)
+    if args.config:
+        return run_config(args)
     if args.kernels_only:
         import torch
         import stmg

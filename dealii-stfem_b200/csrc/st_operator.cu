@@ -91,6 +91,14 @@ namespace stmg
 #undef STMG_SH
       throw Error(STMG_ERR_UNSUPPORTED, "operator: unsupported dim/degree");
     }
+
+    // a small tile is worth taking over a partly filled GPU of big tiles
+    // only while it holds four cells or more
+    bool
+    small_shape_worthwhile(int dim, const int *T3)
+    {
+      return T3[0] * T3[1] * (dim == 3 ? T3[2] : 1) >= 4;
+    }
   } // namespace
 
   std::size_t
@@ -114,7 +122,10 @@ namespace stmg
         if (smem_bytes(T3, nt_in_, nt_out_, elem) <= budget)
           {
             // on small meshes the big tiles leave SMs idle: prefer the small
-            // shape when the big one yields fewer than two tiles per SM
+            // shape when the big one yields fewer than two tiles per SM and
+            // the small one still gives each CTA several cells (a one-cell
+            // tile keeps only nt_out threads of a CTA busy in phase B, far
+            // slower than a partly filled GPU of big tiles)
             if (big && make_tiling(mesh->v, T3).n_tiles < 2ll * sm_count())
               {
                 int t3[3];
@@ -122,7 +133,7 @@ namespace stmg
                   shape_of<double>(mesh->v.dim, mesh->v.p, false, t3);
                 else
                   shape_of<float>(mesh->v.dim, mesh->v.p, false, t3);
-                if (smem_bytes(t3, nt_in_, nt_out_, elem) <= budget)
+                if (small_shape_worthwhile(mesh->v.dim, t3) && smem_bytes(t3, nt_in_, nt_out_, elem) <= budget)
                   continue;
               }
             big_out = big;
@@ -240,7 +251,8 @@ namespace stmg
       shape_of<T>(m.dim, m.p, true, big_sh);
       shape_of<T>(m.dim, m.p, false, small_sh);
       const bool big_fits = smem(big_sh) <= budget, small_fits = smem(small_sh) <= budget;
-      if (big_fits && !(make_tiling(m, big_sh).n_tiles < 2ll * sm_count() && small_fits))
+      if (big_fits && !(make_tiling(m, big_sh).n_tiles < 2ll * sm_count() && small_fits &&
+                        small_shape_worthwhile(m.dim, small_sh)))
         {
           big_out = true;
           return make_tiling(m, big_sh);

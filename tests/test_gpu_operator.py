@@ -23,6 +23,9 @@ CASES = [
     (3, (4, 3, 3), 2, 0.15, 2, (orc.CGP, 2, 2)),
     (3, (3, 3, 2), 3, 0.2, 1, (orc.DG, 2, 1)),
     (3, (2, 2, 2), 4, 0.0, 1, (orc.DG, 1, 1)),
+    # several big tiles of degree 3 and 4 (shell faces and the plane fix-up)
+    (3, (9, 5, 3), 3, 0.2, 1, (orc.DG, 2, 1)),
+    (3, (5, 5, 3), 4, 0.1, 1, (orc.DG, 1, 1)),
     # undistorted boxes with a coefficient per quadrature point
     (2, (6, 5), 2, 0.0, 2, (orc.DG, 1, 2)),
     (3, (5, 4, 3), 2, 0.0, 2, (orc.DG, 3, 1)),
