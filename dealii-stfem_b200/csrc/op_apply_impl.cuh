@@ -311,6 +311,203 @@ namespace stmg
         sweep<P1, DIM, 1, false, true>(qt.S, b, out);
     }
 
+    // Phase B for 3-D cells of degree 3 by planes. The per-thread form
+    // keeps five 64-value arrays live per (cell, time dof) item and spills;
+    // here a group of P1 = 4 consecutive lanes takes one item, lane pz
+    // holding the item's P1 x P1 values in the plane z = pz. Sweeps along x
+    // and y stay in the lane's registers, sweeps along z gather the plane
+    // values of the group by shuffles. w holds the lane's row (or column)
+    // of the 1-D matrix: out[xy] (+)= sum_k w[k] in_k[xy], in_k the value of
+    // the group's lane k.
+    template <int P1, bool ADD, typename T>
+    __device__ __forceinline__ void
+    zsweep(const T (&w)[P1], const T *in, T *out, int gbase)
+    {
+#pragma unroll
+      for (int xy = 0; xy < P1 * P1; ++xy)
+        {
+          T v[P1];
+#pragma unroll
+          for (int k = 0; k < P1; ++k)
+            v[k] = __shfl_sync(0xffffffffu, in[xy], gbase + k);
+          T acc = ADD ? out[xy] : T(0);
+#pragma unroll
+          for (int k = 0; k < P1; ++k)
+            acc += w[k] * v[k];
+          out[xy] = acc;
+        }
+    }
+
+    // K a + M b of one item by planes (lane pz of the group at gbase):
+    // MODE 1 the separable Cartesian form (kappa already in a), MODE 2 the
+    // box cell with a coefficient per cell or quadrature point, MODE 0 the
+    // Q1-mapped cell. a and b hold the plane's nodal values on entry; the
+    // result is left in b.
+    template <int P, typename T, int MODE>
+    __device__ __forceinline__ void
+    planes_apply(const MeshView &m, const QTab<T> &qt, const Cart1D<T> &c1, int cx, int cy, int cz, long long cell,
+                 int pz, int gbase, T *a, T *b)
+    {
+      constexpr int P1 = P + 1;
+      constexpr int PL = P1 * P1;
+      if constexpr (MODE == 1)
+        {
+          // (a, b) <- (M_d a, M_d b + K_d a) along z, y, then x (a dropped)
+          T mz[P1], kz[P1];
+#pragma unroll
+          for (int k = 0; k < P1; ++k)
+            {
+              mz[k] = c1.M[2][pz * P1 + k];
+              kz[k] = c1.K[2][pz * P1 + k];
+            }
+#pragma unroll
+          for (int xy = 0; xy < PL; ++xy)
+            {
+              T va[P1], vb[P1];
+#pragma unroll
+              for (int k = 0; k < P1; ++k)
+                {
+                  va[k] = __shfl_sync(0xffffffffu, a[xy], gbase + k);
+                  vb[k] = __shfl_sync(0xffffffffu, b[xy], gbase + k);
+                }
+              T ma = T(0), sb = T(0);
+#pragma unroll
+              for (int k = 0; k < P1; ++k)
+                {
+                  ma += mz[k] * va[k];
+                  sb += mz[k] * vb[k] + kz[k] * va[k];
+                }
+              a[xy] = ma;
+              b[xy] = sb;
+            }
+#pragma unroll
+          for (int d = 1; d >= 0; --d)
+            {
+              const int stride = d == 0 ? 1 : P1;
+#pragma unroll
+              for (int o = 0; o < P1; ++o)
+                {
+                  const int base = d == 0 ? o * P1 : o;
+                  T         va[P1], vb[P1];
+#pragma unroll
+                  for (int k = 0; k < P1; ++k)
+                    {
+                      va[k] = a[base + k * stride];
+                      vb[k] = b[base + k * stride];
+                    }
+#pragma unroll
+                  for (int i = 0; i < P1; ++i)
+                    {
+                      T ma = T(0), sb = T(0);
+#pragma unroll
+                      for (int k = 0; k < P1; ++k)
+                        {
+                          const T mik = c1.M[d][i * P1 + k];
+                          if (d == 1)
+                            ma += mik * va[k];
+                          sb += mik * vb[k] + c1.K[d][i * P1 + k] * va[k];
+                        }
+                      if (d == 1)
+                        a[base + i * stride] = ma;
+                      b[base + i * stride] = sb;
+                    }
+                }
+            }
+        }
+      else
+        {
+          T sr[P1], sc[P1], dr[P1], dc[P1];
+#pragma unroll
+          for (int k = 0; k < P1; ++k)
+            {
+              sr[k] = qt.S[pz * P1 + k];
+              sc[k] = qt.S[k * P1 + pz];
+              dr[k] = qt.Dq[pz * P1 + k];
+              dc[k] = qt.Dq[k * P1 + pz];
+            }
+          // values at the quadrature points (plane pz is now qz = pz)
+          sweep<P1, 2, 0, false, false>(qt.S, a, a);
+          sweep<P1, 2, 1, false, false>(qt.S, a, a);
+          zsweep<P1, false>(sr, a, a, gbase);
+          sweep<P1, 2, 0, false, false>(qt.S, b, b);
+          sweep<P1, 2, 1, false, false>(qt.S, b, b);
+          zsweep<P1, false>(sr, b, b, gbase);
+          // reference gradients by collocation
+          T g0[PL], g1[PL], g2[PL];
+          sweep<P1, 2, 0, false, false>(qt.Dq, a, g0);
+          sweep<P1, 2, 1, false, false>(qt.Dq, a, g1);
+          zsweep<P1, false>(dr, a, g2, gbase);
+          const T *cq    = nullptr;
+          T        kcell = T(1);
+          if constexpr (sizeof(T) == 8)
+            {
+              if (m.coeff_mode == 1)
+                kcell = T(m.coeff64[cell]);
+              else if (m.coeff_mode == 2)
+                cq = reinterpret_cast<const T *>(m.coeff64) + cell * (PL * P1) + pz * PL;
+            }
+          else
+            {
+              if (m.coeff_mode == 1)
+                kcell = T(m.coeff32[cell]);
+              else if (m.coeff_mode == 2)
+                cq = reinterpret_cast<const T *>(m.coeff32) + cell * (PL * P1) + pz * PL;
+            }
+          const T wz = qt.gw[pz];
+          if constexpr (MODE == 2)
+            {
+              const T det = T(m.h[0]) * T(m.h[1]) * T(m.h[2]);
+              const T ih0 = T(1) / (T(m.h[0]) * T(m.h[0])), ih1 = T(1) / (T(m.h[1]) * T(m.h[1])),
+                      ih2 = T(1) / (T(m.h[2]) * T(m.h[2]));
+#pragma unroll
+              for (int xy = 0; xy < PL; ++xy)
+                {
+                  const int qx = xy % P1, qy = xy / P1;
+                  const T   JxW = det * (qt.gw[qx] * qt.gw[qy] * wz);
+                  const T   kw  = (cq ? cq[xy] : kcell) * JxW;
+                  g0[xy] *= kw * ih0;
+                  g1[xy] *= kw * ih1;
+                  g2[xy] *= kw * ih2;
+                  b[xy] *= JxW;
+                }
+            }
+          else
+            {
+              const T gz = qt.gx[pz];
+              T       X[8][3];
+              load_corners<3>(m, cx, cy, cz, X);
+#pragma unroll
+              for (int xy = 0; xy < PL; ++xy)
+                {
+                  const int qx = xy % P1, qy = xy / P1;
+                  T         xi[3] = {qt.gx[qx], qt.gx[qy], gz};
+                  T         J[3][3], Ji[3][3];
+                  q1_jacobian<3>(X, xi, J);
+                  const T det = det_inv<3>(J, Ji);
+                  const T JxW = fabs(det) * (qt.gw[qx] * qt.gw[qy] * wz);
+                  const T k   = (cq ? cq[xy] : kcell) * JxW;
+                  // physical gradient Ji^T g, flux = k Ji (Ji^T g)
+                  const T gr[3] = {g0[xy], g1[xy], g2[xy]};
+                  T       ph[3];
+#pragma unroll
+                  for (int i = 0; i < 3; ++i)
+                    ph[i] = k * (Ji[0][i] * gr[0] + Ji[1][i] * gr[1] + Ji[2][i] * gr[2]);
+                  g0[xy] = Ji[0][0] * ph[0] + Ji[0][1] * ph[1] + Ji[0][2] * ph[2];
+                  g1[xy] = Ji[1][0] * ph[0] + Ji[1][1] * ph[1] + Ji[1][2] * ph[2];
+                  g2[xy] = Ji[2][0] * ph[0] + Ji[2][1] * ph[1] + Ji[2][2] * ph[2];
+                  b[xy] *= JxW;
+                }
+            }
+          // integrate: collocation derivatives transposed, then S^T
+          sweep<P1, 2, 0, true, true>(qt.Dq, g0, b);
+          sweep<P1, 2, 1, true, true>(qt.Dq, g1, b);
+          zsweep<P1, true>(dc, g2, b, gbase);
+          sweep<P1, 2, 0, false, true>(qt.S, b, b);
+          sweep<P1, 2, 1, false, true>(qt.S, b, b);
+          zsweep<P1, false>(sc, b, b, gbase);
+        }
+    }
+
     // compile-time tile shape per (dim, degree, precision); the fallback
     // shape serves time dimensions whose bricks do not fit the main one
     template <int DIM, int P, typename T, bool BIG>
@@ -346,6 +543,8 @@ namespace stmg
       constexpr int ND = S::ND;
       constexpr int P1 = P + 1;
       constexpr int NW = 8; // warps per CTA
+      // 3-D degree 3: phase B by planes (see planes_apply)
+      constexpr bool PLANES = DIM == 3 && P == 3;
       extern __shared__ __align__(16) unsigned char smem_raw[];
       const int nti = tm.nt_in, nto = tm.nt_out;
       const int ntp = NTPC == 4 ? (nti + 3) / 4 * 4 : NTPC;
@@ -404,6 +603,65 @@ namespace stmg
 
           // B. per (output time dof, cell)
           const T *brick = bricks[buf];
+          if constexpr (PLANES)
+            {
+              // groups of P1 lanes per item; every lane of a warp runs each
+              // pass (the z sweeps shuffle across the warp), lanes without an
+              // item work on the tile's first cell and store nothing
+              constexpr int IPW = 32 / P1;
+              const int     grp = lane / P1, pz = lane - grp * P1, gbase = grp * P1;
+              for (int w0 = warp * IPW; w0 < nto * S::TC; w0 += NW * IPW)
+                {
+                  const int w  = w0 + grp;
+                  int       lc = w / nto, j = w - lc * nto;
+                  int       lx = lc % TX, ly = (lc / TX) % TY, lz = lc / (TX * TY);
+                  const bool item = w < nto * S::TC && lx < tc[0] && ly < tc[1] && lz < tc[2];
+                  if (!item)
+                    lc = j = lx = ly = lz = 0;
+                  const int       cx = c0[0] + lx, cy = c0[1] + ly, cz = c0[2] + lz;
+                  const long long cell = cx + (long long)m.n[0] * (cy + (long long)m.n[1] * cz);
+                  T               kap  = T(1);
+                  if (MODE == 1 && m.coeff_mode == 1)
+                    kap = sizeof(T) == 8 ? T(m.coeff64[cell]) : T(m.coeff32[cell]);
+                  T a[P1 * P1], b[P1 * P1];
+#pragma unroll
+                  for (int q = 0; q < P1 * P1; ++q)
+                    a[q] = b[q] = T(0);
+                  const T *brp = brick + (lx * P + S::E0 * (ly * P + S::E1 * (lz * P + pz))) * ntp;
+                  for (int i0 = 0; i0 < ntp; i0 += NTPC)
+                    {
+                      T al[NTPC], be[NTPC];
+#pragma unroll
+                      for (int u = 0; u < NTPC; ++u)
+                        {
+                          const int i = i0 + u;
+                          al[u]       = i < nti ? tm.A[j * nti + i] * kap : T(0);
+                          be[u]       = i < nti ? tm.B[j * nti + i] : T(0);
+                        }
+#pragma unroll
+                      for (int q = 0; q < P1 * P1; ++q)
+                        {
+                          const T *x = brp + ((q % P1) + S::E0 * (q / P1)) * ntp + i0;
+#pragma unroll
+                          for (int u = 0; u < NTPC; ++u)
+                            {
+                              const T xv = x[u];
+                              a[q] += al[u] * xv;
+                              b[q] += be[u] * xv;
+                            }
+                        }
+                    }
+                  planes_apply<P, T, MODE>(m, qt, c1, cx, cy, cz, cell, pz, gbase, a, b);
+                  if (item)
+                    {
+                      T *cb = cellbuf + (lc * nto + j) * ND + pz * P1 * P1;
+#pragma unroll
+                      for (int q = 0; q < P1 * P1; ++q)
+                        cb[q] = b[q];
+                    }
+                }
+            }
+          else
           for (int w = threadIdx.x; w < nto * S::TC; w += blockDim.x)
             {
               // consecutive threads take the time dofs of one cell: they
