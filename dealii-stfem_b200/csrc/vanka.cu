@@ -784,8 +784,10 @@ namespace stmg
     rec_bytes              = int(pad(mu_off + nd * (compute == STMG_F64 ? 8 : 4)));
     // compile-time tile shape: the streamed apply takes the main shape when
     // two CTAs per SM fit, else the fallback; the other apply also sizes its
-    // record chunk within a shared-memory budget
-    streamed = compute == STMG_F32 && nt <= 4;
+    // record chunk within a shared-memory budget. 3-D cells of degree 3 and
+    // up take the chunked apply: their records (16.6 KB and more) leave the
+    // streamed ring room for one cell per colour phase, one busy warp per CTA.
+    streamed = compute == STMG_F32 && nt <= 4 && !(dim == 3 && p >= 3);
     bool ok  = false;
     for (bool b : {true, false})
       {

@@ -23,6 +23,8 @@ VANKA_CASES = [
     (3, (3, 3, 2), 2, 0.0, True, (orc.DG, 3, 1, orc.HEAT)),
     (3, (4, 3, 3), 2, 0.2, True, (orc.DG, 2, 1, orc.HEAT)),
     (3, (2, 2, 2), 3, 0.15, True, (orc.DG, 2, 1, orc.WAVE)),
+    # degree 3 over several tiles (chunked apply for every precision)
+    (3, (5, 4, 3), 3, 0.2, True, (orc.DG, 2, 1, orc.HEAT)),
 ]
 
 
