@@ -413,7 +413,9 @@ def run_config(args):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
+        torch.cuda.nvtx.range_push(f"timed_slabs_{vname}")  # lets a profiler restrict itself to these slabs
         its = s.run(args.steps)
+        torch.cuda.nvtx.range_pop()
         e1.record()
         torch.cuda.synchronize()
         t = e0.elapsed_time(e1) / 1e3
