@@ -1,5 +1,6 @@
 // Slab solve on the GPU (see solver.h).
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -945,6 +946,9 @@ namespace stmg
     int    it          = 0;
     double reduced_tol = -1;
     bool   first       = true;
+    // second Gram-Schmidt pass: off until a norm check asks for it, then on
+    // for the rest of this solve (deal.II's iterated_gram_schmidt)
+    bool   reorth      = false;
     std::vector<const double *> vp(basis), zp(basis);
     for (int i = 0; i < basis; ++i)
       {
@@ -977,14 +981,30 @@ namespace stmg
           {
             P(Z[j].ptr, V[j].ptr);
             A(aux.ptr, Z[j].ptr);
-            // classical Gram-Schmidt, twice, in three passes over the basis:
-            // h = V^T w; w -= V h with h2 = V^T w on the way; w -= V h2
-            std::vector<double> h(j + 1), h2(j + 1);
-            blas.multidot<double>(n, j + 1, vp.data(), aux.ptr, h.data(), s);
-            blas.orth_update<double>(n, j + 1, h.data(), vp.data(), aux.ptr, h2.data(), s);
-            const double hn2 = blas.orth_update<double>(n, j + 1, h2.data(), vp.data(), aux.ptr, nullptr, s);
+            // classical Gram-Schmidt as deal.II's iterated_gram_schmidt: one
+            // pass over the basis for h = V^T w, one for w -= V h and |w|^2.
+            // Every fifth inner iteration |w|^2 before the pass comes with h
+            // (w dotted with itself); if the pass leaves less than
+            // 10 sqrt(eps) of that norm, a second pass runs now and in every
+            // later iteration of this solve.
+            const bool consider = !reorth && j % 5 == 4;
+            std::vector<double> h(j + 2), h2(j + 1);
+            std::vector<const double *> vw(vp.begin(), vp.begin() + j + 1);
+            if (consider)
+              vw.push_back(aux.ptr);
+            blas.multidot<double>(n, int(vw.size()), vw.data(), aux.ptr, h.data(), s);
+            double hn2 = blas.orth_update<double>(n, j + 1, h.data(), vp.data(), aux.ptr, nullptr, s);
             for (int i = 0; i <= j; ++i)
-              H[i][j] = h[i] + h2[i];
+              H[i][j] = h[i];
+            if (consider && !(std::sqrt(hn2) > 10.0 * std::sqrt(h[j + 1]) * std::sqrt(DBL_EPSILON)))
+              reorth = true;
+            if (reorth)
+              {
+                blas.multidot<double>(n, j + 1, vp.data(), aux.ptr, h2.data(), s);
+                hn2 = blas.orth_update<double>(n, j + 1, h2.data(), vp.data(), aux.ptr, nullptr, s);
+                for (int i = 0; i <= j; ++i)
+                  H[i][j] += h2[i];
+              }
             const double hn = std::sqrt(hn2);
             H[j + 1][j]     = hn;
             if (hn != 0.0)
