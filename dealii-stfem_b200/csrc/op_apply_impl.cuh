@@ -514,7 +514,7 @@ namespace stmg
     struct OpShape
     {
       static constexpr int TX = DIM == 2 ? (P <= 2 ? (BIG ? 16 : 4) : (P <= 4 ? (BIG ? 8 : 2) : (BIG ? 4 : 1)))
-                                         : (P == 1 ? (BIG ? 8 : 2) : (P == 2 ? (BIG ? (sizeof(T) == 4 ? 8 : 4) : 4) : (BIG ? 4 : 1)));
+                                         : (P == 1 ? (BIG ? 8 : 2) : (P == 2 ? (BIG ? 8 : 4) : (BIG ? 4 : 1)));
       static constexpr int TY = DIM == 2 ? TX : (P == 1 ? TX : (P == 2 ? 4 : (BIG ? (P == 3 ? 4 : 2) : 1)));
       static constexpr int TZ = DIM == 2 ? 1 : (P == 1 ? TX : (P == 2 ? (BIG ? 4 : 2) : (BIG ? 2 : 1)));
     };
