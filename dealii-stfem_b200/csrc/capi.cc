@@ -499,6 +499,24 @@ extern "C"
   }
 
   int
+  stmg_solver_solution_async(stmg_solver_t solver, double *u, double *v, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_solution_async: null handle");
+      solver->s->download_async(u, v, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_solver_solution_wait(stmg_solver_t solver)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_solution_wait: null handle");
+      solver->s->download_wait();
+    });
+  }
+
+  int
   stmg_solver_solve(stmg_solver_t solver, double *x, const double *rhs, int *iterations, void *stream)
   {
     return guard([&] {

@@ -1174,6 +1174,7 @@ namespace stmg
         hu[i] = u0 ? u0[i] : su;
         hv[i] = v0 ? v0[i] : sv;
       }
+    wait_snapshot_host();
     STMG_CUDA(cudaMemset(x.ptr, 0, N * nb * 8));
     STMG_CUDA(cudaMemset(v.ptr, 0, N * nb * 8));
     STMG_CUDA(cudaMemcpy(x.ptr + (nb - 1) * N, hu.data(), N * 8, cudaMemcpyHostToDevice));
@@ -1229,6 +1230,7 @@ namespace stmg
   void
   SlabSolver::run(int n_slabs, int *its, cudaStream_t s)
   {
+    wait_snapshot(s);
     const auto                type = tfe::Type(cfg.time_type);
     const std::vector<double> tq   = tfe::basis_points(type, cfg.time_degree);
     for (int slab = 0; slab < n_slabs; ++slab)
@@ -1382,6 +1384,7 @@ namespace stmg
   {
     STMG_REQUIRE(cfg.problem == 1, STMG_ERR_UNSUPPORTED, "gradient: heat problems only");
     STMG_REQUIRE(n_slabs >= 1 && obs && grad, STMG_ERR_ARG, "gradient: bad arguments");
+    wait_snapshot(s);
     Mesh           &fine = *meshes.back();
     STMG_REQUIRE(fine.v.coeff_mode != 2, STMG_ERR_UNSUPPORTED, "gradient: needs a coefficient per cell");
     const long long n    = N * nb;
@@ -1473,6 +1476,74 @@ namespace stmg
       STMG_CUDA(cudaMemcpy(u, x.ptr, N * nb * 8, cudaMemcpyDeviceToHost));
     if (vv)
       STMG_CUDA(cudaMemcpy(vv, v.ptr, N * nb * 8, cudaMemcpyDeviceToHost));
+  }
+
+  SlabSolver::AsyncCopy::~AsyncCopy()
+  {
+    // best effort at teardown: no exceptions out of a destructor
+    if (stream)
+      {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+      }
+    for (cudaEvent_t e : {ready, snapped, copied})
+      if (e)
+        cudaEventDestroy(e);
+  }
+
+  void
+  SlabSolver::download_async(double *u, double *vv, cudaStream_t s)
+  {
+    if (!acopy.stream)
+      {
+        // non-blocking: the legacy default stream must not wait for it
+        STMG_CUDA(cudaStreamCreateWithFlags(&acopy.stream, cudaStreamNonBlocking));
+        STMG_CUDA(cudaEventCreateWithFlags(&acopy.ready, cudaEventDisableTiming));
+        STMG_CUDA(cudaEventCreateWithFlags(&acopy.snapped, cudaEventDisableTiming));
+        STMG_CUDA(cudaEventCreateWithFlags(&acopy.copied, cudaEventDisableTiming));
+      }
+    const std::size_t n = std::size_t(N) * nb;
+    if (u && stage_u.n < n)
+      stage_u.alloc(n);
+    if (vv && stage_v.n < n)
+      stage_v.alloc(n);
+    // device snapshot after the work queued on s, then the host copies; the
+    // copy stream is in order, so a previous host copy out of the staging
+    // buffers has finished before they are overwritten
+    STMG_CUDA(cudaEventRecord(acopy.ready, s));
+    STMG_CUDA(cudaStreamWaitEvent(acopy.stream, acopy.ready, 0));
+    if (u)
+      STMG_CUDA(cudaMemcpyAsync(stage_u.ptr, x.ptr, n * 8, cudaMemcpyDeviceToDevice, acopy.stream));
+    if (vv)
+      STMG_CUDA(cudaMemcpyAsync(stage_v.ptr, v.ptr, n * 8, cudaMemcpyDeviceToDevice, acopy.stream));
+    STMG_CUDA(cudaEventRecord(acopy.snapped, acopy.stream));
+    if (u)
+      STMG_CUDA(cudaMemcpyAsync(u, stage_u.ptr, n * 8, cudaMemcpyDeviceToHost, acopy.stream));
+    if (vv)
+      STMG_CUDA(cudaMemcpyAsync(vv, stage_v.ptr, n * 8, cudaMemcpyDeviceToHost, acopy.stream));
+    STMG_CUDA(cudaEventRecord(acopy.copied, acopy.stream));
+    acopy.pending = true;
+  }
+
+  void
+  SlabSolver::wait_snapshot(cudaStream_t s)
+  {
+    if (acopy.pending)
+      STMG_CUDA(cudaStreamWaitEvent(s, acopy.snapped, 0));
+  }
+
+  void
+  SlabSolver::wait_snapshot_host()
+  {
+    if (acopy.pending)
+      STMG_CUDA(cudaEventSynchronize(acopy.snapped));
+  }
+
+  void
+  SlabSolver::download_wait()
+  {
+    if (acopy.pending)
+      STMG_CUDA(cudaEventSynchronize(acopy.copied));
   }
 
 } // namespace stmg

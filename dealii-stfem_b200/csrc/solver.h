@@ -125,6 +125,14 @@ namespace stmg
     int  solve(double *x, const double *rhs, cudaStream_t s);
     void system_vmult(double *dst, const double *src, cudaStream_t s);
     void download(double *u, double *v) const;
+    // download without a host wait: the last slab's u (and v) blocks are
+    // copied on `s` into device staging buffers, then to the host arrays on
+    // a non-blocking copy stream, so the host transfer overlaps later slabs
+    // (run() waits only for the device copy). download_wait() returns once
+    // the host arrays hold the values; pinned host arrays make the copy
+    // asynchronous.
+    void download_async(double *u, double *v, cudaStream_t s);
+    void download_wait();
     // Heat only: runs n_slabs slabs from the current state and returns the
     // misfit J = 1/2 sum_s |U_s - O_s|^2 (obs: host, n_slabs x n_t x N) and
     // dJ/d(log kappa_c) per fine cell (grad: host), by the discrete adjoint
@@ -155,6 +163,23 @@ namespace stmg
     std::vector<int>                    last_iterations;
 
   private:
+    // copy stream and events of download_async (created on first use)
+    struct AsyncCopy
+    {
+      cudaStream_t stream = nullptr;
+      cudaEvent_t  ready = nullptr, snapped = nullptr, copied = nullptr;
+      bool         pending = false;
+      AsyncCopy()                             = default;
+      AsyncCopy(const AsyncCopy &)            = delete;
+      AsyncCopy &operator=(const AsyncCopy &) = delete;
+      ~AsyncCopy();
+    };
+    DevBuf<double> stage_u, stage_v; // declared first: the copy stream is drained before they go
+    AsyncCopy      acopy;
+    // the work queued on s, or the host, waits for a pending download's
+    // device copy before x and v change
+    void wait_snapshot(cudaStream_t s);
+    void wait_snapshot_host();
     void force(double t, double *out, cudaStream_t s);
     void accumulate_errors(const std::vector<double> &tq, cudaStream_t s);
     DevBuf<double> err_buf, err_num;

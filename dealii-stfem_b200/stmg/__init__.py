@@ -281,6 +281,16 @@ class Solver:
         check(lib().stmg_solver_solution(self.h, _ptr(u), _ptr(v)))
         return u, v
 
+    def solution_async(self, u, v=None, stream=None):
+        """Starts copying the last slab's blocks into the host arrays u (and
+        v), which should be pinned; the copy overlaps later run() calls and
+        is complete after solution_wait(). The arrays must stay alive until
+        then."""
+        check(lib().stmg_solver_solution_async(self.h, _ptr(u), _ptr(v), _stream(stream)))
+
+    def solution_wait(self):
+        check(lib().stmg_solver_solution_wait(self.h))
+
     def solve(self, x, rhs, stream=None):
         k = C.c_int()
         check(lib().stmg_solver_solve(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(rhs.data_ptr()), C.byref(k),

@@ -185,6 +185,15 @@ STMG_API int stmg_solver_set_source(stmg_solver_t solver, const double *f_nodal)
 STMG_API int stmg_solver_run(stmg_solver_t solver, int n_slabs, int *iterations, void *stream);
 /* copy the last slab's u (and v) blocks to host arrays of n_blocks x n_nodes */
 STMG_API int stmg_solver_solution(stmg_solver_t solver, double *u, double *v);
+/* the same copy without a host wait (the caller's solution vector read back
+ * between slabs, time_integrators.h:174-180 and tests/tp_01.cc:630-683): the
+ * blocks are copied on `stream` into device staging buffers and from there to
+ * the host arrays on the library's own non-blocking stream, so the transfer
+ * overlaps the next slabs (stmg_solver_run waits only for the device copy).
+ * The host arrays hold the values once stmg_solver_solution_wait returns;
+ * pinned host memory makes the copy asynchronous. */
+STMG_API int stmg_solver_solution_async(stmg_solver_t solver, double *u, double *v, void *stream);
+STMG_API int stmg_solver_solution_wait(stmg_solver_t solver);
 /* SolverFGMRES::solve of the slab system (time_integrators.h:174) on device
  * vectors x (initial guess in, solution out) and rhs */
 STMG_API int stmg_solver_solve(stmg_solver_t solver, double *x, const double *rhs, int *iterations, void *stream);

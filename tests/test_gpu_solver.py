@@ -186,3 +186,34 @@ def test_gpu_c1_plain_fp64_matches_oracle():
     assert linf == pytest.approx(ref["linf"], rel=1e-6)
     assert l2 == pytest.approx(ref["l2"], rel=1e-6)
     assert h1 == pytest.approx(ref["h1"], rel=1e-6)
+
+
+@pytest.mark.parametrize("problem", ["heat", "wave"])
+def test_gpu_solution_async_matches_blocking_copy(problem):
+    """stmg_solver_solution_async: the host arrays hold the slab the copy was
+    started after, although the next slabs run (and overwrite the device
+    solution) before the wait; equal to the blocking copy bit for bit."""
+    import stmg
+    kw = dict(dim=2, refine=3, degree=2, time_degree=1, time_type=stmg.DG, n_steps=1, fe_degree_min=0,
+              n_steps_min=1, problem=stmg.HEAT if problem == "heat" else stmg.WAVE)
+    ref = stmg.Solver(**kw)
+    ref.run(1)
+    u1, v1 = ref.solution()
+    ref.run(1)
+    u2, v2 = ref.solution()
+    s = stmg.Solver(**kw)
+    n = s.n_blocks * s.n_nodes
+    hu = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    hv = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    hu[:] = np.nan
+    hv[:] = np.nan
+    s.run(1)
+    s.solution_async(hu, hv)
+    s.run(2)  # moves the device solution on while the copy may still run
+    s.solution_wait()
+    assert np.array_equal(hu, u1) and np.array_equal(hv, v1)
+    s2 = stmg.Solver(**kw)
+    s2.run(2)
+    s2.solution_async(hu)
+    s2.solution_wait()
+    assert np.array_equal(hu, u2)
