@@ -1,7 +1,7 @@
 // Oracle (test infrastructure only): CPU FP64 restatement of the reference's
 // time finite-element algebra, tests/include/fe_time.h of nlsmrg/dealii-stfem.
 // Only tests/, the bench's CPU-baseline leg and the smoke check use this code,
-// and only as the checker; the product never links it.
+// and only to check results against; the product never links it.
 #pragma once
 
 #include <array>

@@ -1,6 +1,6 @@
 """ctypes access to the CPU oracle (oracle/build/liboracle.so).
 
-Test infrastructure only: the oracle is the checker the CUDA path is compared
+Test infrastructure only: the oracle is what the CUDA path is compared
 against; nothing in the product imports this module.
 """
 import ctypes as C
