@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <utility>
 
 #include "kernels_common.cuh"
 #include "op_apply_impl.cuh"
@@ -973,6 +974,9 @@ namespace stmg
         STMG_REQUIRE(it < max_iter, STMG_ERR_NOCONV, "fgmres: iteration limit reached");
         std::vector<std::vector<double>> H(basis + 1, std::vector<double>(basis, 0.0));
         std::vector<double>              cs(basis), sn(basis), g(basis + 1, 0.0);
+        // V[i] holds the i-th basis vector divided by sc[i]: a new direction
+        // keeps the orthogonalised w itself (buffer swap, no normalising pass)
+        std::vector<double> sc(basis, 1.0);
         g[0] = beta;
         axpby<double>(n, 1.0 / beta, aux.ptr, 0.0, V[0].ptr, s);
         int  used = 0;
@@ -987,28 +991,41 @@ namespace stmg
             // (w dotted with itself); if the pass leaves less than
             // 10 sqrt(eps) of that norm, a second pass runs now and in every
             // later iteration of this solve.
+            // With the stored scales: h_i = sc_i (V[i] . w), w -= sum_i (h_i sc_i) V[i].
             const bool consider = !reorth && j % 5 == 4;
-            std::vector<double> h(j + 2), h2(j + 1);
+            std::vector<double> h(j + 2), h2(j + 1), c(j + 1);
             std::vector<const double *> vw(vp.begin(), vp.begin() + j + 1);
             if (consider)
               vw.push_back(aux.ptr);
             blas.multidot<double>(n, int(vw.size()), vw.data(), aux.ptr, h.data(), s);
-            double hn2 = blas.orth_update<double>(n, j + 1, h.data(), vp.data(), aux.ptr, nullptr, s);
             for (int i = 0; i <= j; ++i)
-              H[i][j] = h[i];
+              {
+                h[i] *= sc[i];
+                c[i]    = h[i] * sc[i];
+                H[i][j] = h[i];
+              }
+            double hn2 = blas.orth_update<double>(n, j + 1, c.data(), vp.data(), aux.ptr, nullptr, s);
             if (consider && !(std::sqrt(hn2) > 10.0 * std::sqrt(h[j + 1]) * std::sqrt(DBL_EPSILON)))
               reorth = true;
             if (reorth)
               {
                 blas.multidot<double>(n, j + 1, vp.data(), aux.ptr, h2.data(), s);
-                hn2 = blas.orth_update<double>(n, j + 1, h2.data(), vp.data(), aux.ptr, nullptr, s);
                 for (int i = 0; i <= j; ++i)
-                  H[i][j] += h2[i];
+                  {
+                    h2[i] *= sc[i];
+                    c[i] = h2[i] * sc[i];
+                    H[i][j] += h2[i];
+                  }
+                hn2 = blas.orth_update<double>(n, j + 1, c.data(), vp.data(), aux.ptr, nullptr, s);
               }
             const double hn = std::sqrt(hn2);
             H[j + 1][j]     = hn;
             if (hn != 0.0)
-              axpby<double>(n, 1.0 / hn, aux.ptr, 0.0, V[j + 1].ptr, s);
+              {
+                std::swap(V[j + 1], aux);
+                vp[j + 1] = V[j + 1].ptr;
+                sc[j + 1] = 1.0 / hn;
+              }
             for (int i = 0; i < j; ++i)
               {
                 const double t = cs[i] * H[i][j] + sn[i] * H[i + 1][j];
