@@ -14,8 +14,10 @@ The JSON line carries the device-timed throughput (`value`), the end-to-end
 throughput through the C ABI with host buffers (`e2e`), the all-FP64
 V-cycle throughput on the same workload (`fp64_mg`), the roofline of the
 finest-level operator and Vanka kernels timed in isolation, the CPU oracle
-baseline on a bounded sample, clocks sampled during the timed region and the
-number of kernels launched.
+baseline on a bounded sample, clocks sampled during the timed region, the
+number of kernels launched and (`accuracy`) the per-slab relative difference
+of the FP32-MG and all-FP64 solutions from a converged all-FP64 solve of the
+same 8 slabs.
 """
 import argparse
 import json
@@ -102,19 +104,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one
+# finest-level FP32 Vanka apply, from an ncu capture of the same kernel on
+# 64^3 Q2 cells with n_t = 4 (the records exceed L2 there, and the traffic
+# grows with the cell count): python bench.py --kernels-only vanka_apply
+# --refine 6 under ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum.
+VANKA_TRAFFIC_PER_CELL = 3523.76
+
+
 def vanka_traffic(refine):
-    """DRAM bytes (read + write) of one finest-level Vanka apply from the
-    committed ncu summary (captured on 64^3 cells and scaled by the cell
-    count, traffic growing with the cells), or None."""
-    path = os.path.join(REPO, "profiles", "vanka_apply_64cube.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_cell:"):
-                    return float(line.split(":")[1]) * (1 << refine) ** 3
-    except (OSError, ValueError):
-        pass
-    return None
+    """DRAM bytes of one finest-level Vanka apply on (2^refine)^3 cells."""
+    return VANKA_TRAFFIC_PER_CELL * (1 << refine) ** 3
 
 
 def peaks():
@@ -211,6 +211,44 @@ def replica_throughput(world, dofs_per_step, steps, t):
     return world * dofs_per_step * steps / t
 
 
+# relative residual of the converged FP64 solve the accuracy figures compare
+# against (the FP64 FGMRES stagnates near 1e-13 on these systems)
+ACC_REF_TOL = 1e-12
+
+
+def slab_solutions(solver, w, n_slabs):
+    """The solver's solution blocks after each of n_slabs slabs run from a
+    zero initial state (host FP64 arrays); untimed."""
+    out = []
+    if n_slabs:
+        solver.set_initial(np.zeros(w["nodes"]))
+        for _ in range(n_slabs):
+            solver.run(1)
+            u, _ = solver.solution(want_v=False)
+            out.append(u)
+    return out
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def accuracy_report(u32, u64, uref, tol):
+    """Per-slab relative 2-norm differences of the FP32-MG solve (u32) and
+    the all-FP64 solve (u64), both to `tol`, against a converged all-FP64
+    solve (uref, ACC_REF_TOL), and of u32 against u64."""
+    rep = dict(reference=f"all-FP64 multigrid, FGMRES to {ACC_REF_TOL:g} relative residual", slabs=len(uref),
+               fp32_mg_vs_reference=[_rel(a, r) for a, r in zip(u32, uref)])
+    if u64:
+        rep["fp64_mg_vs_reference"] = [_rel(a, r) for a, r in zip(u64, uref)]
+        rep["fp32_mg_vs_fp64_mg"] = [_rel(a, b) for a, b in zip(u32, u64)]
+    rep["max_fp32_mg_vs_reference"] = max(rep["fp32_mg_vs_reference"])
+    rep["target"] = 1e-7
+    rep["meets_target"] = rep["max_fp32_mg_vs_reference"] <= 1e-7
+    rep["solver_tol"] = tol
+    return rep
+
+
 def kernel_roofline(stmg, torch, w, kappa, hbm, only=None, fp64=False):
     """Finest-level FP32 operator and Vanka apply timed in isolation with CUDA
     events on the launching stream; algorithmic bytes per launch:
@@ -266,10 +304,12 @@ def run_ours(args):
     kappa, f = inputs(w, SEED + rank)
     hbm, hbm_kind = peaks()
 
-    def make(mg_dtype):
+    def make(mg_dtype, tol=w["tol"], max_iter=200):
         return stmg.Solver(dim=3, refine=w["refine"], degree=2, time_degree=3, time_type=stmg.DG,
-                           problem=stmg.HEAT, n_steps=1, tau=w["tau"], mg_dtype=mg_dtype, tol=w["tol"],
-                           abs_tol=1e-300, rhs_mode=1, f_nodal=f, fine_coeff=kappa)
+                           problem=stmg.HEAT, n_steps=1, tau=w["tau"], mg_dtype=mg_dtype, tol=tol,
+                           abs_tol=1e-300, rhs_mode=1, f_nodal=f, fine_coeff=kappa, max_iter=max_iter)
+
+    n_acc = 0 if args.no_accuracy else w["n_slabs"]
 
     def timed(solver, steps, warmup):
         solver.set_initial(np.zeros(w["nodes"]))
@@ -323,18 +363,29 @@ def run_ours(args):
     te = time.perf_counter() - te
     e2e = dict(value=world * dofs_step * args.steps / te, unit="DoF/s", h2d_bytes_per_step=w["nodes"] * 8,
                d2h_bytes_per_step=w["nt"] * w["nodes"] * 8)
+    u32 = slab_solutions(solver, w, n_acc)
     del solver
     torch.cuda.empty_cache()
 
-    fp64 = None
+    fp64, u64 = None, []
     if not args.no_fp64:
         s64 = make(stmg.F64)
         t64, its64, _ = timed(s64, args.steps, min(args.warmup, 1))
         fp64 = dict(value=world * dofs_step * args.steps / t64, ms_per_step=1e3 * t64 / args.steps,
                     fgmres_iterations=[int(i) for i in its64],
                     speedup_fp32_mg=(world * dofs_step * args.steps / t32) / (world * dofs_step * args.steps / t64))
+        u64 = slab_solutions(s64, w, n_acc)
         del s64
         torch.cuda.empty_cache()
+
+    accuracy = None
+    if n_acc:
+        sref = make(stmg.F64, tol=ACC_REF_TOL, max_iter=1000)
+        uref = slab_solutions(sref, w, n_acc)
+        del sref
+        torch.cuda.empty_cache()
+        accuracy = accuracy_report(u32, u64, uref, w["tol"])
+    del u32, u64
 
     kr = kernel_roofline(stmg, torch, w, kappa, hbm)
     dom = max(kr, key=lambda k: kr[k]["ms"])
@@ -357,7 +408,7 @@ def run_ours(args):
                                 tol=w["tol"], l2="inputs larger than L2 (FGMRES basis 30 x 0.54 GB)",
                                 parallelism="replicas" if world > 1 else "single-gpu", setup_s=t_setup),
                     fgmres_iterations=[int(i) for i in its32], e2e=e2e, roofline=roof, cpu_baseline=cpu,
-                    clocks=clk, gpu_launches=int(launches), fp64_mg=fp64)
+                    clocks=clk, gpu_launches=int(launches), fp64_mg=fp64, accuracy=accuracy)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -373,7 +424,10 @@ def run_config(args):
       c2  3-D 32^3 Q3, vertices moved +-0.2h, kappa = 10^U(-2,2), dG(2),
           dt 1/32, f = 1: FP32 vs FP64 multigrid;
       c3  3-D wave 64^3 Q2, c^2 in {0.5, 1, 4}, dG(2), dt 1/128, Gaussian
-          pulse, v0 = 0, f = 0: Vanka stored in FP32 vs BF16."""
+          pulse, v0 = 0, f = 0: Vanka stored in FP32 vs BF16.
+    For c2 and c3 a converged all-FP64 solve of the same slabs is run last
+    and the line's `accuracy` gives each variant's relative difference from
+    it after the last slab."""
     import torch
     import meshes
     import stmg
@@ -407,9 +461,12 @@ def run_config(args):
                     fine_coeff=c2)
         variants = {"fp32-vanka": dict(mg_dtype=stmg.F32, vanka_storage=stmg.F32),
                     "bf16-vanka": dict(mg_dtype=stmg.F32, vanka_storage=stmg.BF16)}
-    out = {}
+    if args.config != "c1":
+        # a converged all-FP64 solve of the same slabs, for the accuracy figures
+        variants["reference"] = dict(mg_dtype=stmg.F64, tol=ACC_REF_TOL, max_iter=1000)
+    out, sols = {}, {}
     for vname, vkw in variants.items():
-        s = stmg.Solver(**base, **vkw)
+        s = stmg.Solver(**{**base, **vkw})
         if init is not None:
             s.set_initial(*init)
         s.run(args.warmup)
@@ -427,11 +484,23 @@ def run_config(args):
                      fgmres_iterations=[int(i) for i in its])
         if args.config == "c1":
             entry["errors"] = dict(zip(("linf", "l2", "h1"), s.errors()))
+        else:
+            sols[vname] = s.solution(want_v=False)[0]
         out[vname] = entry
         del s
         torch.cuda.empty_cache()
-    print(json.dumps(dict(workload=name, steps=args.steps, warmup=args.warmup, slabs=args.warmup + args.steps,
-                          variants=out)), flush=True)
+    line = dict(workload=name, steps=args.steps, warmup=args.warmup, slabs=args.warmup + args.steps, variants=out)
+    if sols:
+        # relative 2-norm difference of each variant's last slab solution
+        # (after warmup + steps slabs from the same initial state) from the
+        # converged all-FP64 solve
+        ref = sols.pop("reference")
+        line["accuracy"] = dict(reference=f"all-FP64 multigrid, FGMRES to {ACC_REF_TOL:g} relative residual",
+                                target=1e-7, **{f"{k}_vs_reference": _rel(u, ref) for k, u in sols.items()})
+        if len(sols) == 2:
+            (ka, ua), (kb, ub) = sols.items()
+            line["accuracy"][f"{ka}_vs_{kb}"] = _rel(ua, ub)
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -494,6 +563,9 @@ def main():
     ap.add_argument("--refine", type=int, default=7, help="mesh 2^refine cells per direction (7: 128^3)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 V-cycle comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the per-slab comparison of the FP32-MG and FP64-MG solutions with a converged "
+                         "FP64 solve")
     ap.add_argument("--kernels-only", choices=["all", "st_apply", "st_apply64", "vanka_apply"], default=None,
                     help="only time the finest-level operator (FP32 or FP64) and/or Vanka apply in isolation "
                          "(profiling)")

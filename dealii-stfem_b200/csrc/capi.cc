@@ -167,6 +167,23 @@ extern "C"
   }
 
   int
+  stmg_time_transfer(int time_type, int kind, int r, int n_steps, double *P)
+  {
+    return guard([&] {
+      STMG_REQUIRE(time_type == 1 || time_type == 2, STMG_ERR_ARG, "time_transfer: time type 1 (cGP) or 2 (dG)");
+      STMG_REQUIRE(kind == 0 || kind == 1, STMG_ERR_ARG, "time_transfer: kind 0 (k projection) or 1 (tau)");
+      STMG_REQUIRE(n_steps >= 1 && P, STMG_ERR_ARG, "time_transfer: bad steps or null output");
+      STMG_REQUIRE(kind == 1 || r >= (time_type == 2 ? 1 : 2), STMG_ERR_ARG,
+                   "time_transfer: the k projection needs a coarse degree r - 1 of the time type");
+      STMG_REQUIRE(kind == 0 || (n_steps % 2 == 0 && r >= (time_type == 2 ? 0 : 1)), STMG_ERR_ARG,
+                   "time_transfer: the tau prolongation needs an even step count");
+      const auto      t = tfe::Type(time_type);
+      const tfe::Mat  M = kind == 0 ? tfe::projection(t, r - 1, r, n_steps) : tfe::prolongation(t, r, n_steps);
+      std::copy(M.a.begin(), M.a.end(), P);
+    });
+  }
+
+  int
   stmg_mesh_create(int dim, const int *n_cells, int degree, const double *lo, const double *hi, const double *vertices,
                    int coeff_mode, const double *coeff, stmg_mesh_t *mesh)
   {

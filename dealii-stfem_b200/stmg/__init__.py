@@ -92,6 +92,20 @@ def time_weights(time_type, r, tau, n_steps, problem=HEAT):
     return A, B, rK, rM, rV
 
 
+def time_transfer(time_type, kind, r, n_steps):
+    """Time transfer matrix of one slab (stmg_time_transfer): kind 0 the
+    k-projection r-1 -> r on n_steps steps, kind 1 the tau-prolongation
+    n_steps/2 -> n_steps steps; rows are the fine time dofs."""
+    per = r + 1 if time_type == DG else r
+    if kind == 0:
+        shape = (per * n_steps, (per - 1) * n_steps)
+    else:
+        shape = (per * n_steps, per * n_steps // 2)
+    P = np.zeros(shape)
+    check(lib().stmg_time_transfer(time_type, kind, r, n_steps, _ptr(P)))
+    return P
+
+
 class Mesh:
     """stmg_mesh_t: structured FE_Q(p) mesh level on the device."""
 

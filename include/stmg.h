@@ -68,6 +68,15 @@ STMG_API int stmg_kernel_launches(long long *count);
 STMG_API int stmg_time_weights(int time_type, int r, double tau, int n_steps, int problem, double *Alpha,
                                double *Beta, double *rK, double *rM, double *rV);
 
+/* Time transfer matrix of one slab (rows = fine time dofs, row-major):
+ * kind 0, the k-projection from degree r-1 to r on n_steps steps
+ * (get_time_projection_matrix, fe_time.h:567-623; (r n_steps) x
+ * ((r-1) n_steps) for cGP, ((r+1) n_steps) x (r n_steps) for dG);
+ * kind 1, the tau-prolongation from n_steps/2 to n_steps steps of degree r
+ * (get_time_prolongation_matrix, fe_time.h:625-669; n_steps even). The
+ * restriction is the transpose (gmg.h:77-136 with restrict_is_transpose). */
+STMG_API int stmg_time_transfer(int time_type, int kind, int r, int n_steps, double *P);
+
 /* ---------------------------------------------------------------- mesh
  * Structured hex mesh of n_cells[0] x n_cells[1] (x n_cells[2]) cells of
  * FE_Q(degree) on Gauss-Lobatto nodes with MappingQ1 and homogeneous
