@@ -9,16 +9,45 @@ namespace stmg
 {
   namespace
   {
-    constexpr int RED_BLOCKS  = 592; // 4 x 148 SMs
+    constexpr int RED_BLOCKS  = 592; // 4 x 148 SMs: the grid of a large reduction
     constexpr int RED_THREADS = 256;
 
-    // Block sums of cnt per-thread values acc[0..cnt) into partial[blockIdx.x * cnt + i]:
-    // warp shuffles, then one thread per value over the warps (fixed order).
+    // Reduction grid for n entries: about four entries per thread, at most
+    // RED_BLOCKS blocks (small vectors take a few blocks, so their partial
+    // sums are few).
+    unsigned
+    red_grid(long long n)
+    {
+      const long long b = (n + 4 * RED_THREADS - 1) / (4 * RED_THREADS);
+      return unsigned(b < 1 ? 1 : (b > RED_BLOCKS ? RED_BLOCKS : b));
+    }
+
+    // What the last block does with the cnt reduced values r_i: with
+    // nscale > 0, h_i = r_i sc_i and c_i = h_i sc_i for i < nscale (the
+    // Gram-Schmidt coefficients of basis vectors stored divided by sc_i; c
+    // stays on the device for the update pass); every value goes to out (a
+    // mapped pinned host buffer).
+    struct Finish
+    {
+      double       *out;
+      double       *c;
+      int           nscale;
+      Coeffs        sc;
+      unsigned     *counter;
+    };
+
+    // Block sums of cnt per-thread values acc[0..cnt) into partial[blockIdx.x * cnt + i]
+    // (warp shuffles, then one thread per value over the warps, fixed order);
+    // the block that finishes last reduces all blocks' partials (each value
+    // by one warp: lanes take blocks lane, lane + 32, ..., then a shuffle
+    // tree) and applies `fin`. The order depends on the grid only, so the
+    // result is reproducible bit for bit.
     template <int MAXV>
     __device__ __forceinline__ void
-    block_sums(double (&acc)[MAXV], int cnt, double *partial)
+    block_sums(double (&acc)[MAXV], int cnt, double *partial, const Finish &fin)
     {
       __shared__ double sh[RED_THREADS / 32][MAXV];
+      __shared__ bool   last;
       const int         lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
       for (int i = 0; i < MAXV; ++i)
@@ -40,12 +69,41 @@ namespace stmg
             t += sh[w][threadIdx.x];
           partial[blockIdx.x * cnt + threadIdx.x] = t;
         }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0)
+        last = atomicAdd(fin.counter, 1u) == gridDim.x - 1;
+      __syncthreads();
+      if (!last)
+        return;
+      const int nb = gridDim.x;
+      for (int i = warp; i < cnt; i += RED_THREADS / 32)
+        {
+          double t = 0;
+          for (int b = lane; b < nb; b += 32)
+            t += __ldcg(partial + b * cnt + i);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1)
+            t += __shfl_xor_sync(0xffffffffu, t, o);
+          if (lane == 0)
+            {
+              if (i < fin.nscale)
+                {
+                  t *= fin.sc.c[i];
+                  fin.c[i] = t * fin.sc.c[i];
+                }
+              fin.out[i] = t;
+            }
+        }
+      if (threadIdx.x == 0)
+        *fin.counter = 0u; // ready for the next reduction on this stream
     }
 
     // partial[b * m + i] = block b's share of V_i . w; w is read once
     template <typename T, int MAXV>
     __global__ void __launch_bounds__(RED_THREADS)
-    multidot_partial(long long n, int m, const __grid_constant__ VecPtrs V, const T *__restrict__ w, double *partial)
+    multidot_partial(long long n, int m, const __grid_constant__ VecPtrs V, const T *__restrict__ w, double *partial,
+                     const __grid_constant__ Finish fin)
     {
       double acc[MAXV];
 #pragma unroll
@@ -59,51 +117,34 @@ namespace stmg
             if (i < m)
               acc[i] += double(__ldg(static_cast<const T *>(V.p[i]) + k)) * wk;
         }
-      block_sums<MAXV>(acc, m, partial);
+      block_sums<MAXV>(acc, m, partial, fin);
     }
 
-    // w -= sum_i c_i V_i; partial sums of w_new . w_new, then (if dots) of
-    // V_i . w_new, with the V_i[k] kept in registers between the two uses
+    // w -= sum_i c_i V_i with c on the device (written by the multidot's last
+    // block); partial sums of w_new . w_new
     template <typename T, int MAXV>
     __global__ void __launch_bounds__(RED_THREADS)
-    orth_update_kernel(long long n, int m, const __grid_constant__ Coeffs c, const __grid_constant__ VecPtrs V,
-                       T *__restrict__ w, int dots, double *partial)
+    orth_update_kernel(long long n, int m, const double *__restrict__ cdev, const __grid_constant__ VecPtrs V,
+                       T *__restrict__ w, double *partial, const __grid_constant__ Finish fin)
     {
-      double acc[MAXV + 1];
+      double c[MAXV];
 #pragma unroll
-      for (int i = 0; i <= MAXV; ++i)
-        acc[i] = 0;
+      for (int i = 0; i < MAXV; ++i)
+        c[i] = i < m ? cdev[i] : 0.0;
+      double acc[1] = {0.0};
       for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
         {
-          double v[MAXV];
           double s = double(w[k]);
 #pragma unroll
           for (int i = 0; i < MAXV; ++i)
-            {
-              v[i] = i < m ? double(__ldg(static_cast<const T *>(V.p[i]) + k)) : 0.0;
-              s -= c.c[i] * v[i];
-            }
+            if (i < m)
+              s -= c[i] * double(__ldg(static_cast<const T *>(V.p[i]) + k));
           const T st = T(s);
           w[k]       = st;
           const double sw = double(st);
           acc[0] += sw * sw;
-#pragma unroll
-          for (int i = 0; i < MAXV; ++i)
-            acc[i + 1] += v[i] * sw;
         }
-      block_sums<MAXV + 1>(acc, dots ? m + 1 : 1, partial);
-    }
-
-    __global__ void
-    reduce_partials(int nblocks, int m, const double *partial, double *out)
-    {
-      const int i = threadIdx.x;
-      if (i >= m)
-        return;
-      double s = 0;
-      for (int b = 0; b < nblocks; ++b)
-        s += partial[b * m + i];
-      out[i] = s;
+      block_sums<1>(acc, 1, partial, fin);
     }
 
     // w = alpha * w + sum_i c_i V_i   (c in kernel parameters)
@@ -122,12 +163,14 @@ namespace stmg
         }
     }
 
+    // y = Tout(scale x); scale is a power of two (or 1), so the product is
+    // exact and the conversion rounds as without it
     template <typename Tout, typename Tin>
     __global__ void
-    convert_kernel(long long n, const Tin *__restrict__ x, Tout *__restrict__ y)
+    convert_kernel(long long n, const Tin *__restrict__ x, Tout *__restrict__ y, double scale)
     {
       for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-        y[k] = Tout(x[k]);
+        y[k] = Tout(double(x[k]) * scale);
     }
 
     // y = a x + b y
@@ -167,8 +210,11 @@ namespace stmg
   Blas::Blas()
   {
     partial.alloc(std::size_t(RED_BLOCKS) * (MAX_DOTS + 1));
-    result.alloc(MAX_DOTS + 1);
-    STMG_CUDA(cudaMallocHost(&host_result, (MAX_DOTS + 1) * sizeof(double)));
+    coef.alloc(MAX_DOTS + 1);
+    counter.alloc(1);
+    STMG_CUDA(cudaMemset(counter.ptr, 0, sizeof(unsigned)));
+    STMG_CUDA(cudaHostAlloc(&host_result, (MAX_DOTS + 2) * sizeof(double), cudaHostAllocMapped));
+    STMG_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&dev_result), host_result, 0));
   }
 
   Blas::~Blas()
@@ -177,17 +223,31 @@ namespace stmg
       cudaFreeHost(host_result);
   }
 
-  // reduce the block partials of m values and copy them to out (host)
+  template <typename T>
   void
-  Blas::fetch(int m, double *out, cudaStream_t s)
+  Blas::launch_multidot(long long n, int m, const T *const *V, const T *w, int nscale, const double *sc,
+                        double *out_dev, cudaStream_t s)
   {
-    reduce_partials<<<1, 64, 0, s>>>(RED_BLOCKS, m, partial.ptr, result.ptr);
+    STMG_REQUIRE(m >= 1 && m <= MAX_DOTS, STMG_ERR_ARG, "multidot: 1..32 vectors");
+    VecPtrs vp{};
+    for (int i = 0; i < m; ++i)
+      vp.p[i] = V[i];
+    Finish fin{};
+    fin.out     = out_dev;
+    fin.c       = coef.ptr;
+    fin.nscale  = nscale;
+    fin.counter = reinterpret_cast<unsigned *>(counter.ptr);
+    for (int i = 0; i < nscale; ++i)
+      fin.sc.c[i] = sc[i];
+    const unsigned g = red_grid(n);
+    if (m <= 8)
+      multidot_partial<T, 8><<<g, RED_THREADS, 0, s>>>(n, m, vp, w, partial.ptr, fin);
+    else if (m <= 16)
+      multidot_partial<T, 16><<<g, RED_THREADS, 0, s>>>(n, m, vp, w, partial.ptr, fin);
+    else
+      multidot_partial<T, MAX_DOTS><<<g, RED_THREADS, 0, s>>>(n, m, vp, w, partial.ptr, fin);
     count_launch();
     STMG_CUDA(cudaGetLastError());
-    STMG_CUDA(cudaMemcpyAsync(host_result, result.ptr, m * sizeof(double), cudaMemcpyDeviceToHost, s));
-    STMG_CUDA(cudaStreamSynchronize(s));
-    for (int i = 0; i < m; ++i)
-      out[i] = host_result[i];
   }
 
   template <typename T>
@@ -195,18 +255,10 @@ namespace stmg
   Blas::multidot(long long n, int m, const T *const *V, const T *w, double *out, cudaStream_t s)
   {
     STMG_REQUIRE(m >= 1 && m <= MAX_DOTS, STMG_ERR_ARG, "multidot: 1..32 vectors");
-    VecPtrs vp{};
+    launch_multidot<T>(n, m, V, w, 0, nullptr, dev_result, s);
+    STMG_CUDA(cudaStreamSynchronize(s));
     for (int i = 0; i < m; ++i)
-      vp.p[i] = V[i];
-    if (m <= 8)
-      multidot_partial<T, 8><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, vp, w, partial.ptr);
-    else if (m <= 16)
-      multidot_partial<T, 16><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, vp, w, partial.ptr);
-    else
-      multidot_partial<T, 32><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, vp, w, partial.ptr);
-    count_launch();
-    STMG_CUDA(cudaGetLastError());
-    fetch(m, out, s);
+      out[i] = host_result[i];
   }
 
   template <typename T>
@@ -238,38 +290,45 @@ namespace stmg
 
   template <typename T>
   double
-  Blas::orth_update(long long n, int m, const double *c, const T *const *V, T *w, double *dots, cudaStream_t s)
+  Blas::gs_pass(long long n, int m, const T *const *V, const double *sc, T *w, bool with_self, double *h,
+                cudaStream_t s)
   {
-    STMG_REQUIRE(m >= 1 && m <= MAX_DOTS, STMG_ERR_ARG, "orth_update: 1..32 vectors");
-    Coeffs  cc{};
+    STMG_REQUIRE(m >= 1 && m <= MAX_DOTS, STMG_ERR_ARG, "gs_pass: 1..32 basis vectors");
+    const T *vw[MAX_DOTS + 1];
+    for (int i = 0; i < m; ++i)
+      vw[i] = V[i];
+    vw[m]        = w;
+    const int md = with_self ? m + 1 : m;
+    STMG_REQUIRE(md <= MAX_DOTS, STMG_ERR_ARG, "gs_pass: basis plus self dot beyond 32 vectors");
+    // h_i = sc_i (V_i . w), c_i = h_i sc_i (and w . w), reduced by the last block
+    launch_multidot<T>(n, md, vw, w, m, sc, dev_result, s);
+    // w -= sum_i c_i V_i with the c_i left on the device; w . w after the update
     VecPtrs vp{};
     for (int i = 0; i < m; ++i)
-      {
-        cc.c[i] = c[i];
-        vp.p[i] = V[i];
-      }
-    const int d = dots ? 1 : 0;
+      vp.p[i] = V[i];
+    Finish fin{};
+    fin.out        = dev_result + MAX_DOTS + 1;
+    fin.counter    = reinterpret_cast<unsigned *>(counter.ptr);
+    const unsigned g = red_grid(n);
     if (m <= 8)
-      orth_update_kernel<T, 8><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, cc, vp, w, d, partial.ptr);
+      orth_update_kernel<T, 8><<<g, RED_THREADS, 0, s>>>(n, m, coef.ptr, vp, w, partial.ptr, fin);
     else if (m <= 16)
-      orth_update_kernel<T, 16><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, cc, vp, w, d, partial.ptr);
+      orth_update_kernel<T, 16><<<g, RED_THREADS, 0, s>>>(n, m, coef.ptr, vp, w, partial.ptr, fin);
     else
-      orth_update_kernel<T, 32><<<RED_BLOCKS, RED_THREADS, 0, s>>>(n, m, cc, vp, w, d, partial.ptr);
+      orth_update_kernel<T, MAX_DOTS><<<g, RED_THREADS, 0, s>>>(n, m, coef.ptr, vp, w, partial.ptr, fin);
     count_launch();
     STMG_CUDA(cudaGetLastError());
-    double out[MAX_DOTS + 1];
-    fetch(dots ? m + 1 : 1, out, s);
-    if (dots)
-      for (int i = 0; i < m; ++i)
-        dots[i] = out[i + 1];
-    return out[0];
+    STMG_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < md; ++i)
+      h[i] = host_result[i];
+    return host_result[MAX_DOTS + 1];
   }
 
   template <typename Tout, typename Tin>
   void
-  convert(long long n, const Tin *x, Tout *y, cudaStream_t s)
+  convert(long long n, const Tin *x, Tout *y, cudaStream_t s, double scale)
   {
-    convert_kernel<Tout, Tin><<<grid_for(n), 256, 0, s>>>(n, x, y);
+    convert_kernel<Tout, Tin><<<grid_for(n), 256, 0, s>>>(n, x, y, scale);
     count_launch();
     STMG_CUDA(cudaGetLastError());
   }
@@ -305,15 +364,15 @@ namespace stmg
   template void   Blas::multidot<T>(long long, int, const T *const *, const T *, double *, cudaStream_t);  \
   template double Blas::dot<T>(long long, const T *, const T *, cudaStream_t);                              \
   template void   Blas::combine<T>(long long, double, int, const double *, const T *const *, T *, cudaStream_t); \
-  template double Blas::orth_update<T>(long long, int, const double *, const T *const *, T *, double *, cudaStream_t); \
+  template double Blas::gs_pass<T>(long long, int, const T *const *, const double *, T *, bool, double *, cudaStream_t); \
   template void   axpby<T>(long long, T, const T *, T, T *, cudaStream_t);                                  \
   template void   sub_from<T>(long long, const T *, T *, cudaStream_t);                                     \
   template void   fill<T>(long long, T, T *, cudaStream_t);
   STMG_BLAS_INST(double)
   STMG_BLAS_INST(float)
 #undef STMG_BLAS_INST
-  template void convert<float, double>(long long, const double *, float *, cudaStream_t);
-  template void convert<double, float>(long long, const float *, double *, cudaStream_t);
-  template void convert<double, double>(long long, const double *, double *, cudaStream_t);
-  template void convert<float, float>(long long, const float *, float *, cudaStream_t);
+  template void convert<float, double>(long long, const double *, float *, cudaStream_t, double);
+  template void convert<double, float>(long long, const float *, double *, cudaStream_t, double);
+  template void convert<double, double>(long long, const double *, double *, cudaStream_t, double);
+  template void convert<float, float>(long long, const float *, float *, cudaStream_t, double);
 } // namespace stmg

@@ -19,7 +19,8 @@ namespace stmg
   };
 
   // Reductions with FP64 accumulation in a fixed order; owns its scratch
-  // (block partial sums and a pinned result), allocated once.
+  // (block partial sums, a completion counter, the Gram-Schmidt coefficients
+  // and a mapped pinned result buffer), allocated once. One stream at a time.
   class Blas
   {
   public:
@@ -36,19 +37,26 @@ namespace stmg
     // w = alpha w + sum_i c_i V_i
     template <typename T>
     void combine(long long n, double alpha, int m, const double *c, const T *const *V, T *w, cudaStream_t s);
-    // one Gram-Schmidt update in a single pass: w -= sum_i c_i V_i, then
-    // dots[i] = V_i . w (if dots) and returns w . w (synchronises)
+    // One classical Gram-Schmidt pass against basis vectors stored divided
+    // by sc_i: h_i = sc_i (V_i . w) for i < m (and h_m = w . w before the
+    // pass if with_self), then w -= sum_i (h_i sc_i) V_i with the
+    // coefficients kept on the device; returns w . w after the update.
+    // Two kernels and one host wait (synchronises the stream).
     template <typename T>
-    double orth_update(long long n, int m, const double *c, const T *const *V, T *w, double *dots, cudaStream_t s);
+    double gs_pass(long long n, int m, const T *const *V, const double *sc, T *w, bool with_self, double *h,
+                   cudaStream_t s);
 
   private:
-    void fetch(int m, double *out, cudaStream_t s);
-    DevBuf<double> partial, result;
-    double        *host_result = nullptr;
+    template <typename T>
+    void launch_multidot(long long n, int m, const T *const *V, const T *w, int nscale, const double *sc,
+                         double *out_dev, cudaStream_t s);
+    DevBuf<double> partial, coef, counter;
+    double        *host_result = nullptr, *dev_result = nullptr;
   };
 
+  // y = scale x in the output type; scale must be a power of two (exact)
   template <typename Tout, typename Tin>
-  void convert(long long n, const Tin *x, Tout *y, cudaStream_t s);
+  void convert(long long n, const Tin *x, Tout *y, cudaStream_t s, double scale = 1.0);
   template <typename T>
   void axpby(long long n, T a, const T *x, T b, T *y, cudaStream_t s); // y = a x + b y
   template <typename T>

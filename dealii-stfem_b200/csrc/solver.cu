@@ -872,21 +872,25 @@ namespace stmg
   }
 
   void
-  GMG::vmult(double *dst, const double *src, cudaStream_t s)
+  GMG::vmult(double *dst, const double *src, cudaStream_t s, double scale)
   {
+    // The V-cycle is linear: with scale a power of two, the cycle runs on
+    // scale * src and its result is multiplied by 1 / scale, both exact, so
+    // dst is the same to the last bit while the cycle's vectors keep a
+    // moderate size in its own precision.
     Level          &top = levels.back();
     const long long n   = top.size();
     if (dtype == STMG_F64)
       {
-        convert<double, double>(n, src, as<double>(top.def), s);
+        convert<double, double>(n, src, as<double>(top.def), s, scale);
         cycle<double>(s);
-        convert<double, double>(n, as<double>(top.sol), dst, s);
+        convert<double, double>(n, as<double>(top.sol), dst, s, 1.0 / scale);
       }
     else
       {
-        convert<float, double>(n, src, as<float>(top.def), s);
+        convert<float, double>(n, src, as<float>(top.def), s, scale);
         cycle<float>(s);
-        convert<double, float>(n, as<float>(top.sol), dst, s);
+        convert<double, float>(n, as<float>(top.sol), dst, s, 1.0 / scale);
       }
   }
 
@@ -983,7 +987,11 @@ namespace stmg
         bool done = false;
         for (int j = 0; j + 1 < basis; ++j)
           {
-            P(Z[j].ptr, V[j].ptr);
+            // V[j] has norm 1 / sc[j] (up to rounding); the preconditioner
+            // gets it scaled by the power of two nearest sc[j], so the FP32
+            // V-cycle sees a vector of norm in [1/2, 2) however far the
+            // products of the subdiagonal norms drift over a restart cycle
+            P(Z[j].ptr, V[j].ptr, std::ldexp(1.0, std::ilogb(sc[j] * 1.4142135623730951)));
             A(aux.ptr, Z[j].ptr);
             // classical Gram-Schmidt as deal.II's iterated_gram_schmidt: one
             // pass over the basis for h = V^T w, one for w -= V h and |w|^2.
@@ -992,31 +1000,20 @@ namespace stmg
             // 10 sqrt(eps) of that norm, a second pass runs now and in every
             // later iteration of this solve.
             // With the stored scales: h_i = sc_i (V[i] . w), w -= sum_i (h_i sc_i) V[i].
+            // The coefficients h_i sc_i stay on the device between the two
+            // passes (Blas::gs_pass): one host wait per pass.
             const bool consider = !reorth && j % 5 == 4;
-            std::vector<double> h(j + 2), h2(j + 1), c(j + 1);
-            std::vector<const double *> vw(vp.begin(), vp.begin() + j + 1);
-            if (consider)
-              vw.push_back(aux.ptr);
-            blas.multidot<double>(n, int(vw.size()), vw.data(), aux.ptr, h.data(), s);
+            std::vector<double> h(j + 2), h2(j + 1);
+            double hn2 = blas.gs_pass<double>(n, j + 1, vp.data(), sc.data(), aux.ptr, consider, h.data(), s);
             for (int i = 0; i <= j; ++i)
-              {
-                h[i] *= sc[i];
-                c[i]    = h[i] * sc[i];
-                H[i][j] = h[i];
-              }
-            double hn2 = blas.orth_update<double>(n, j + 1, c.data(), vp.data(), aux.ptr, nullptr, s);
+              H[i][j] = h[i];
             if (consider && !(std::sqrt(hn2) > 10.0 * std::sqrt(h[j + 1]) * std::sqrt(DBL_EPSILON)))
               reorth = true;
             if (reorth)
               {
-                blas.multidot<double>(n, j + 1, vp.data(), aux.ptr, h2.data(), s);
+                hn2 = blas.gs_pass<double>(n, j + 1, vp.data(), sc.data(), aux.ptr, false, h2.data(), s);
                 for (int i = 0; i <= j; ++i)
-                  {
-                    h2[i] *= sc[i];
-                    c[i] = h2[i] * sc[i];
-                    H[i][j] += h2[i];
-                  }
-                hn2 = blas.orth_update<double>(n, j + 1, c.data(), vp.data(), aux.ptr, nullptr, s);
+                  H[i][j] += h2[i];
               }
             const double hn = std::sqrt(hn2);
             H[j + 1][j]     = hn;
@@ -1240,7 +1237,7 @@ namespace stmg
   SlabSolver::solve(double *xv, const double *b, cudaStream_t s)
   {
     auto Aop = [&](double *dst, const double *src) { A64->apply(false, src, dst, false, s); };
-    auto Pop = [&](double *dst, const double *src) { gmg->vmult(dst, src, s); };
+    auto Pop = [&](double *dst, const double *src, double scale) { gmg->vmult(dst, src, s, scale); };
     return gmres->solve(Aop, Pop, xv, b, cfg.abs_tol, cfg.tol, cfg.max_iter, s);
   }
 
@@ -1445,7 +1442,7 @@ namespace stmg
     STMG_CUDA(cudaMemcpyAsync(x_end.ptr, x.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
     const double t_end = time;
     auto         AT    = [&](double *dst, const double *src) { A64->apply(true, src, dst, false, s); };
-    auto         PT    = [&](double *dst, const double *src) { gmgT->vmult(dst, src, s); };
+    auto         PT    = [&](double *dst, const double *src, double scale) { gmgT->vmult(dst, src, s, scale); };
     bool         have_next = false;
     for (int seg = nseg - 1; seg >= 0; --seg)
       {

@@ -56,7 +56,9 @@ namespace stmg
     GMG(const GMG &)            = delete;
     GMG &operator=(const GMG &) = delete;
     // FP64 in, FP64 out; FP32 or FP64 inside (GMG::vmult, gmg.h:846-859)
-    void vmult(double *dst, const double *src, cudaStream_t s);
+    // dst = V-cycle(src); scale (a power of two) is applied to src before
+    // the cycle and undone after it, exactly
+    void vmult(double *dst, const double *src, cudaStream_t s, double scale = 1.0);
     std::vector<double> omegas() const;
     std::vector<Level>  levels; // coarsest first
     int                 dtype;

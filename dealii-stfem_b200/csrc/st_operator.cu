@@ -107,42 +107,48 @@ namespace stmg
     return op_smem_bytes(mesh->v.dim, mesh->v.p, shape, nt_in_, nt_out_, elem);
   }
 
+  // Tile shape of an operator apply on mesh m with elements of elem bytes:
+  // the big shape unless it does not fit in shared memory, or it yields
+  // fewer than two tiles per SM while the small shape still gives each CTA
+  // several cells (a one-cell tile keeps only nt_out threads of a CTA busy
+  // in phase B, far slower than a partly filled GPU of big tiles). Used by
+  // StOperator and by the allocation-free box apply, so both pick the same.
   Tiling
-  StOperator::choose_tiling(int nt_in_, int nt_out_, bool &big_out, int *shape) const
+  choose_op_tiling(const MeshView &m, std::size_t elem, int nt_in_, int nt_out_, bool &big_out, int *shape)
   {
-    const std::size_t elem   = dtype == STMG_F64 ? 8 : 4;
     const std::size_t budget = 200 * 1024;
+    auto              shp    = [&](bool big, int *T3) {
+      if (elem == 8)
+        shape_of<double>(m.dim, m.p, big, T3);
+      else
+        shape_of<float>(m.dim, m.p, big, T3);
+    };
     for (bool big : {true, false})
       {
         int T3[3];
-        if (dtype == STMG_F64)
-          shape_of<double>(mesh->v.dim, mesh->v.p, big, T3);
-        else
-          shape_of<float>(mesh->v.dim, mesh->v.p, big, T3);
-        if (smem_bytes(T3, nt_in_, nt_out_, elem) <= budget)
+        shp(big, T3);
+        if (op_smem_bytes(m.dim, m.p, T3, nt_in_, nt_out_, elem) <= budget)
           {
-            // on small meshes the big tiles leave SMs idle: prefer the small
-            // shape when the big one yields fewer than two tiles per SM and
-            // the small one still gives each CTA several cells (a one-cell
-            // tile keeps only nt_out threads of a CTA busy in phase B, far
-            // slower than a partly filled GPU of big tiles)
-            if (big && make_tiling(mesh->v, T3).n_tiles < 2ll * sm_count())
+            if (big && make_tiling(m, T3).n_tiles < 2ll * sm_count())
               {
                 int t3[3];
-                if (dtype == STMG_F64)
-                  shape_of<double>(mesh->v.dim, mesh->v.p, false, t3);
-                else
-                  shape_of<float>(mesh->v.dim, mesh->v.p, false, t3);
-                if (small_shape_worthwhile(mesh->v.dim, t3) && smem_bytes(t3, nt_in_, nt_out_, elem) <= budget)
+                shp(false, t3);
+                if (small_shape_worthwhile(m.dim, t3) && op_smem_bytes(m.dim, m.p, t3, nt_in_, nt_out_, elem) <= budget)
                   continue;
               }
             big_out = big;
             for (int d = 0; d < 3; ++d)
               shape[d] = T3[d];
-            return make_tiling(mesh->v, T3);
+            return make_tiling(m, T3);
           }
       }
     throw Error(STMG_ERR_UNSUPPORTED, "operator: time blocks do not fit in shared memory");
+  }
+
+  Tiling
+  StOperator::choose_tiling(int nt_in_, int nt_out_, bool &big_out, int *shape) const
+  {
+    return choose_op_tiling(mesh->v, dtype == STMG_F64 ? 8 : 4, nt_in_, nt_out_, big_out, shape);
   }
 
   StOperator::StOperator(Mesh *mesh_, int nt_out_, int nt_in_, const double *A_, const double *B_, int dtype_)
@@ -240,35 +246,14 @@ namespace stmg
       return scratch_device_ptr[dev];
     }
 
-    // the tiling StOperator::choose_tiling picks for these sizes
-    template <typename T>
-    Tiling
-    box_tiling(const MeshView &m, int nd, int nt_in, int nt_out, bool &big_out)
-    {
-      const std::size_t budget = 200 * 1024;
-      auto              smem   = [&](const int *sh) { return op_smem_bytes(m.dim, m.p, sh, nt_in, nt_out, sizeof(T)); };
-      int big_sh[3], small_sh[3];
-      shape_of<T>(m.dim, m.p, true, big_sh);
-      shape_of<T>(m.dim, m.p, false, small_sh);
-      const bool big_fits = smem(big_sh) <= budget, small_fits = smem(small_sh) <= budget;
-      if (big_fits && !(make_tiling(m, big_sh).n_tiles < 2ll * sm_count() && small_fits &&
-                        small_shape_worthwhile(m.dim, small_sh)))
-        {
-          big_out = true;
-          return make_tiling(m, big_sh);
-        }
-      STMG_REQUIRE(small_fits, STMG_ERR_UNSUPPORTED, "operator: time blocks do not fit in shared memory");
-      big_out = false;
-      return make_tiling(m, small_sh);
-    }
-
     template <typename T>
     void
     box_apply(const MeshView &m, int nd, const double *A, const double *B, int nt_out, int nt_in, const T *src, T *dst,
               cudaStream_t s)
     {
       bool         big = true;
-      const Tiling tl  = box_tiling<T>(m, nd, nt_in, nt_out, big);
+      int          shape[3];
+      const Tiling tl = choose_op_tiling(m, sizeof(T), nt_in, nt_out, big, shape);
       const std::size_t need = tl.n_tiles > 1 ? std::size_t(tl.n_tiles) * nt_out * tl.tile_stride * sizeof(T) : 0;
       if (need > NOALLOC_SCRATCH_BYTES)
         throw Error(STMG_ERR_SHAPE, "op_vmult_box_noalloc: this mesh needs " + std::to_string(need) +
@@ -327,6 +312,7 @@ namespace stmg
           }
       }
     m.cartesian  = 1;
+    m.box        = 1;
     m.vert       = nullptr;
     m.coeff_mode = coeff ? 1 : 0;
     m.coeff64    = dtype == STMG_F64 ? static_cast<const double *>(coeff) : nullptr;

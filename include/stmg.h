@@ -112,12 +112,15 @@ STMG_API int stmg_op_vmult(stmg_op_t op, void *dst, const void *src, void *strea
  * double for STMG_F64), or NULL for 1. dst, src: device, nt x n_nodes.
  * The tiles' face slots go to one fixed 16 MiB array in the library's device
  * code, held on every GPU that loads the library until the process exits;
- * a mesh that needs more returns STMG_ERR_SHAPE (in 3-D with Q2 and four
- * time blocks, meshes up to about 48^3 cells fit). The first call on each
- * device looks up that array's device address on the current device, so
- * make it before any stream capture. All calls share the array: calls
- * that run at the same time on one GPU race. No counterpart in the
- * reference. */
+ * a mesh that needs more (tiles x nt_out x face slots per tile x element
+ * size) returns STMG_ERR_SHAPE: in 3-D with Q2 and four time blocks, meshes
+ * up to about 40^3 cells fit in FP64 and about 52^3 in FP32. The first call
+ * on each device looks up that array's device address on the current
+ * device and keeps it for the life of the process, so make it before any
+ * stream capture, and do not use this entry point on a device after
+ * cudaDeviceReset (the library's device image is then loaded again at
+ * another address). All calls share the array: calls that run at the same
+ * time on one GPU race. No counterpart in the reference. */
 STMG_API int stmg_op_vmult_box_noalloc(int dim, const int *n_cells, int degree, const double *lo, const double *hi,
                                        const void *coeff, int nt_out, int nt_in, const double *A, const double *B,
                                        int dtype, void *dst, const void *src, void *stream);

@@ -39,6 +39,10 @@ def _record(g, total):
         pass
 
 
+# (section, k, refine) of golden configurations whose totals differ from the
+# reference's by rounding of the FP32 V-cycle: none at present
+NEAR_TOTALS = set()
+
 GOLD_CASES = [g for g in _gold() if g["refine"] <= 4 and not (g["refine"] == 4 and g["k"] == 3)]
 
 
@@ -53,8 +57,13 @@ def test_gpu_iterations_match_tp01(g):
     its = s.run(g["slabs"])
     total = int(its.sum())
     _record(g, total)
-    # the parity bar: within one iteration per slab of the reference
-    assert abs(total - g["iterations"]) <= g["slabs"], (total, g["iterations"])
+    # the reference's FGMRES total exactly (every one of these configurations
+    # reproduced it on the B200); a configuration listed in NEAR_TOTALS would
+    # be held to one iteration per slab instead
+    if (g["section"], g["k"], g["refine"]) in NEAR_TOTALS:
+        assert abs(total - g["iterations"]) <= g["slabs"], (total, g["iterations"])
+    else:
+        assert total == g["iterations"], (total, g["iterations"])
     # error norms against the manufactured solution, as printed (6 digits)
     linf, l2, h1 = s.errors()
     assert linf == pytest.approx(g["linf"], rel=2e-5)
@@ -220,3 +229,25 @@ def test_gpu_solution_async_matches_blocking_copy(problem):
     s2.solution_async(hu)
     s2.solution_wait()
     assert np.array_equal(hu, u2)
+
+
+def test_gpu_short_restart_tight_tolerance_fp32_matches_fp64():
+    """FGMRES over several restart cycles (restart 8) to a tight tolerance
+    (1e-12) on the distorted Q3 shape (4^3 cells, kappa = 10^U(-2, 2),
+    dG(2)): each basis vector reaches the FP32 V-cycle scaled by a power of
+    two to a norm near one, so the FP32-multigrid solve converges like the
+    all-FP64 one and the solutions agree."""
+    import stmg
+    n = 4
+    X = meshes.vertices(3, (n, n, n), distort=0.2, seed=51)
+    coeff = meshes.log_uniform(n ** 3, 1e-2, 1e2, seed=52)
+    kw = dict(dim=3, refine=2, degree=3, time_degree=2, time_type=stmg.DG, problem=stmg.HEAT, n_steps=1,
+              tau=1 / 32, rhs_mode=1, f_nodal=np.ones((3 * n + 1) ** 3), fine_coeff=coeff, fine_vertices=X,
+              tol=1e-12, abs_tol=1e-300, restart=8, max_iter=1000)
+    s32 = stmg.Solver(mg_dtype=stmg.F32, **kw)
+    s64 = stmg.Solver(mg_dtype=stmg.F64, **kw)
+    its32, its64 = s32.run(2), s64.run(2)
+    assert its32.max() > 8 and np.all(np.abs(its32 - its64) <= 2), (its32, its64)
+    u32, _ = s32.solution()
+    u64, _ = s64.solution()
+    assert np.linalg.norm(u32 - u64) <= 1e-10 * np.linalg.norm(u64)
