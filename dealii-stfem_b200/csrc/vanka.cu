@@ -23,6 +23,8 @@
 
 #include "kernels_common.cuh"
 #include "vanka.h"
+
+#include <mutex>
 #include "vanka_apply_impl.cuh"
 
 namespace stmg
@@ -88,7 +90,7 @@ namespace stmg
     vanka_setup_kernel(const MeshView m, const double *__restrict__ Kref, const double *__restrict__ Mref,
                        const double *__restrict__ elemK, const double *__restrict__ elemM,
                        unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int mu_double,
-                       int *__restrict__ status, const Tiling tl, int tiled)
+                       int *__restrict__ status, const Tiling tl, int tiled, int row_stride, int mu_stride)
     {
       constexpr int P1 = P + 1;
       constexpr int ND = Tens<P1, DIM>::ND;
@@ -315,15 +317,15 @@ namespace stmg
             }
           unsigned char *mr = rec + slot * rec_bytes + mu_off;
           if (mu_double)
-            reinterpret_cast<double *>(mr)[col] = K[col][col];
+            reinterpret_cast<double *>(mr)[col * mu_stride] = K[col][col];
           else
-            reinterpret_cast<float *>(mr)[col] = float(K[col][col]);
+            reinterpret_cast<float *>(mr)[col * mu_stride] = float(K[col][col]);
         }
       __syncthreads();
       for (int e = tid; e < ND * ND; e += nth)
         {
           const int mm = e / ND, a = e % ND;
-          reinterpret_cast<TS *>(rec + slot * rec_bytes)[e] = to_storage<TS>(Q[a][mm]);
+          reinterpret_cast<TS *>(rec + slot * rec_bytes)[mm * row_stride + a] = to_storage<TS>(Q[a][mm]);
         }
     }
 
@@ -416,6 +418,9 @@ namespace stmg
     if (streamed)
       {
         const std::size_t ntp = nt == 3 ? 4 : nt;
+        if (rowrec)
+          return std::size_t(vanka_detail::VR_STAGES) * colour_cells * rec_bytes +
+                 4 * (3 * nb * ntp + vanka_detail::VR_WARPS * std::size_t(mesh->nd) * ntp);
         return std::size_t(vanka_detail::VK_STAGES) * colour_cells * rec_bytes +
                4 * (3 * nb * ntp + 8 * std::size_t(mesh->nd) * ntp);
       }
@@ -477,7 +482,7 @@ namespace stmg
         (void)Vp;
         kern<<<unsigned(m.ncells), threads, smem>>>(m, Kref.ptr, Mref.ptr, eK.ptr, eM.ptr, vk.V.ptr, vk.rec_bytes,
                                                     vk.mu_off, vk.compute == STMG_F64 ? 1 : 0, status.ptr, vk.tiling,
-                                                    vk.streamed ? 1 : 0);
+                                                    vk.streamed ? 1 : 0, vk.row_stride, vk.mu_stride);
         count_launch();
         STMG_CUDA(cudaGetLastError());
       };
@@ -780,14 +785,45 @@ namespace stmg
     const std::size_t nd   = mesh->nd;
     const std::size_t elem = storage == STMG_F64 ? 8 : (storage == STMG_F32 ? 4 : 2);
     auto              pad  = [](std::size_t b) { return (b + 15) / 16 * 16; };
-    mu_off                 = int(pad(nd * nd * elem));
-    rec_bytes              = int(pad(mu_off + nd * (compute == STMG_F64 ? 8 : 4)));
     // compile-time tile shape: the streamed apply takes the main shape when
     // two CTAs per SM fit, else the fallback; the other apply also sizes its
     // record chunk within a shared-memory budget. 3-D cells of degree 3 and
     // up take the chunked apply: their records (16.6 KB and more) leave the
     // streamed ring room for one cell per colour phase, one busy warp per CTA.
     streamed = compute == STMG_F32 && nt <= 4 && !(dim == 3 && p >= 3);
+    {
+      const char *e = std::getenv("STMG_VANKA_ROWREC");
+      // the row-record kernel is built for the eigenvalue pattern of the
+      // dG / cGP time matrices: one real eigenvalue for odd n_t, none for even
+      int nreal = 0;
+      for (int k = 0; k < nt; ++k)
+        nreal += teig.kind[k] == 1 ? 1 : 0;
+      rowrec = streamed && teig.use && nd <= 32 && nreal == nt % 2 && !(e && e[0] == '0');
+    }
+    if (rowrec)
+      {
+        row_stride = storage == STMG_F32 ? vk_row_stride<float>(int(nd)) : vk_row_stride<__nv_bfloat16>(int(nd));
+        if (storage == STMG_F32)
+          {
+            // mu in the row after the mode's entries
+            mu_off    = int(nd * 4);
+            mu_stride = row_stride;
+            rec_bytes = int(nd * row_stride * 4);
+          }
+        else
+          {
+            mu_off    = int(pad(nd * row_stride * elem));
+            mu_stride = 1;
+            rec_bytes = int(pad(mu_off + nd * 4));
+          }
+      }
+    else
+      {
+        row_stride = int(nd);
+        mu_stride  = 1;
+        mu_off     = int(pad(nd * nd * elem));
+        rec_bytes  = int(pad(mu_off + nd * (compute == STMG_F64 ? 8 : 4)));
+      }
     bool ok  = false;
     for (bool b : {true, false})
       {
@@ -810,7 +846,10 @@ namespace stmg
           }
       }
     if (!ok)
-      streamed = false;
+      {
+        streamed = false;
+        STMG_REQUIRE(!rowrec, STMG_ERR_UNSUPPORTED, "vanka: row records do not fit in shared memory");
+      }
     for (bool b : {true, false})
       {
         if (ok)
@@ -834,6 +873,9 @@ namespace stmg
     const long long slots =
       streamed ? tiling.n_tiles * (long long)tiling.T[0] * tiling.T[1] * tiling.T[2] : mesh->v.ncells;
     V.alloc(std::size_t(slots) * rec_bytes);
+    // record padding (and the slots of cells beyond a partial tile) is read
+    // by whole-row and whole-phase copies: keep it zero
+    STMG_CUDA(cudaMemset(V.ptr, 0, std::size_t(slots) * rec_bytes));
 #define STMG_SETUP(D, PP)                                                                                \
   if (dim == D && p == PP)                                                                               \
     run_setup<D, PP>(*this);
@@ -849,10 +891,43 @@ namespace stmg
     apply_ex(src, dst, 1.0, 0.0, s);
   }
 
+  namespace
+  {
+    std::mutex fault_mutex;
+    int       *fault_host = nullptr, *fault_dev = nullptr;
+
+    void
+    fault_alloc()
+    {
+      std::lock_guard<std::mutex> lock(fault_mutex);
+      if (!fault_host)
+        {
+          STMG_CUDA(cudaHostAlloc(&fault_host, sizeof(int), cudaHostAllocMapped));
+          *fault_host = 0;
+          STMG_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&fault_dev), fault_host, 0));
+        }
+    }
+  } // namespace
+
+  int *
+  vanka_fault_flag_device()
+  {
+    fault_alloc();
+    return fault_dev;
+  }
+
+  void
+  vanka_check_fault()
+  {
+    if (fault_host && *reinterpret_cast<volatile int *>(fault_host))
+      throw Error(STMG_ERR_CUDA, "vanka: a record copy to shared memory did not complete in time (kernel gave up)");
+  }
+
   void
   Vanka::apply_ex(const void *src, void *dst, double alpha, double beta, cudaStream_t s) const
   {
     STMG_REQUIRE(src && dst, STMG_ERR_ARG, "vanka: null vector");
+    vanka_check_fault();
     if (mesh->v.dim == 2)
       return vanka_apply_2d(*this, src, dst, alpha, beta, s);
     return vanka_apply_3d(*this, src, dst, alpha, beta, s);

@@ -20,6 +20,24 @@ namespace stmg
     float G[16], S[16]; // n_t x n_t row-major (n_t <= 4)
   };
 
+  // Row records (the row-record apply, FP32 compute): V as rows of
+  // vk_row_stride elements per mode. FP32 rows hold the mode's nd entries,
+  // then its eigenvalue mu, then zeros (a whole number of 16-byte words per
+  // row); BF16 rows hold the nd entries and zeros (8-byte words), and the FP32
+  // mu values follow the rows.
+  template <typename TS>
+  constexpr int
+  vk_row_stride(int nd)
+  {
+    return sizeof(TS) == 4 ? (nd + 1 + 3) / 4 * 4 : (nd + 3) / 4 * 4;
+  }
+
+  // Set by a Vanka apply kernel whose wait for a record copy gave up (mapped
+  // host memory, read by Vanka::check_fault); 0 while all is well.
+  int *vanka_fault_flag_device();
+  // throws Error(STMG_ERR_CUDA) if a Vanka kernel flagged a failed wait
+  void vanka_check_fault();
+
   class Vanka
   {
   public:
@@ -54,6 +72,12 @@ namespace stmg
     // streamed: FP32 compute with 1..4 time dofs; records are then stored in
     // (tile, colour, cell) order, colour_cells records per colour at most
     bool                  streamed = false;
+    // rowrec: the streamed records in row form (vk_row_stride), applied by
+    // the row-record kernel (time solves in the eigenbasis, nd <= 32);
+    // row_stride = elements per row, mu_stride = elements between successive
+    // mu values from mu_off (in the mu type)
+    bool                  rowrec     = false;
+    int                   row_stride = 0, mu_stride = 1;
     int                   colour_cells = 1;
     bool                  big = true;                // compile-time tile shape in use
     int                   shape[3] = {1, 1, 1};

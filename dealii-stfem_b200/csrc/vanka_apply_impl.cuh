@@ -4,6 +4,8 @@
 
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 #include "tile_ops.cuh"
 #include "vanka.h"
 
@@ -687,6 +689,472 @@ namespace stmg
       cp_async_wait<0>();
     }
 
+    // ------------------------------------------------- row-record apply
+    // Record streaming by the bulk copy engine: one cp.async.bulk (global ->
+    // this CTA's shared memory, no multicast) per colour phase, completing on
+    // an mbarrier. Every wait is bounded: after VR_WAIT_LIMIT polls the
+    // kernel sets the fault flag, waits (bounded) for the copies it issued and
+    // returns.
+    constexpr int       VR_STAGES     = 3;         // record stages (colour phases in flight)
+    constexpr int       VR_WARPS      = 8;         // warps per CTA, a warp per cell
+    constexpr long long VR_WAIT_LIMIT = 1ll << 22; // polls of one barrier phase
+
+    __device__ __forceinline__ unsigned
+    smem_u32(const void *p)
+    {
+      return static_cast<unsigned>(__cvta_generic_to_shared(p));
+    }
+
+    __device__ __forceinline__ void
+    mbar_init(unsigned bar, unsigned count)
+    {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+    }
+
+    __device__ __forceinline__ void
+    mbar_expect_tx(unsigned bar, unsigned bytes)
+    {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+    }
+
+    __device__ __forceinline__ void
+    mbar_arrive(unsigned bar)
+    {
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+    }
+
+    // true once the phase of the given parity has completed, false after
+    // VR_WAIT_LIMIT polls
+    __device__ __forceinline__ bool
+    mbar_wait(unsigned bar, unsigned parity)
+    {
+      for (long long it = 0; it < VR_WAIT_LIMIT; ++it)
+        {
+          unsigned done;
+          asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                       "selp.u32 %0, 1, 0, p;\n}\n"
+                       : "=r"(done)
+                       : "r"(bar), "r"(parity)
+                       : "memory");
+          if (done)
+            return true;
+        }
+      return false;
+    }
+
+    // bytes (a multiple of 16, 16-byte aligned ends) global -> shared,
+    // completing on bar
+    __device__ __forceinline__ void
+    bulk_copy_g2s(unsigned dst, const void *src, unsigned bytes, unsigned bar)
+    {
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+                   "l"(src), "r"(bytes), "r"(bar)
+                   : "memory");
+    }
+
+    // orders this thread's earlier shared-memory accesses before later
+    // bulk-copy writes to the same bytes
+    __device__ __forceinline__ void
+    fence_proxy_async_smem()
+    {
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+
+    // entries a of a row held as 16-byte words (FP32) or 8-byte words (BF16)
+    template <typename TS>
+    struct RowWord
+    {
+      using W = std::conditional_t<sizeof(TS) == 4, float4, uint2>;
+      static constexpr int PER = sizeof(W) / sizeof(TS); // entries per word
+      __device__ __forceinline__ static float
+      get(const W &w, int i)
+      {
+        if constexpr (sizeof(TS) == 4)
+          return i == 0 ? w.x : (i == 1 ? w.y : (i == 2 ? w.z : w.w));
+        else
+          {
+            const unsigned u = (i < 2) ? w.x : w.y;
+            return (i & 1) ? __uint_as_float(u & 0xffff0000u) : __uint_as_float(u << 16);
+          }
+      }
+    };
+
+    // y (NTP values as pairs) += v * x (NTP values)
+    template <int NTP>
+    __device__ __forceinline__ void
+    acc_time(float2 (&y)[(NTP + 1) / 2], float v, const float *x)
+    {
+      if constexpr (NTP == 4)
+        {
+          const float4 q  = *reinterpret_cast<const float4 *>(x);
+          const float2 vv = make_float2(v, v);
+          y[0]            = __ffma2_rn(vv, make_float2(q.x, q.y), y[0]);
+          y[1]            = __ffma2_rn(vv, make_float2(q.z, q.w), y[1]);
+        }
+      else if constexpr (NTP == 2)
+        y[0] = __ffma2_rn(make_float2(v, v), *reinterpret_cast<const float2 *>(x), y[0]);
+      else
+        y[0].x = fmaf(v, *x, y[0].x);
+    }
+
+    // 1 / d to about one ulp (the multifunction unit's reciprocal)
+    __device__ __forceinline__ float
+    rcp_approx(float d)
+    {
+      float r;
+      asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+      return r;
+    }
+
+    // w = (mu Lambda + I)^{-1} y in the real block form of the eigenbasis of
+    // Beta^{-1} Alpha (the G and S factors are applied to whole bricks): NR
+    // real eigenvalues first, then complex pairs (a_k +- i b_k), each pair's
+    // 2x2 block [[mu a + 1, mu b], [-mu b, mu a + 1]] inverted
+    template <int NT, int NR>
+    __device__ __forceinline__ void
+    mode_scale(const TimeEig &te, float mu, float (&y)[NT])
+    {
+#pragma unroll
+      for (int k = 0; k < NR; ++k)
+        y[k] *= rcp_approx(fmaf(mu, te.a[k], 1.0f));
+#pragma unroll
+      for (int k = NR; k + 1 < NT; k += 2)
+        {
+          const float d = fmaf(mu, te.a[k], 1.0f), e = mu * te.b[k];
+          const float inv = rcp_approx(fmaf(d, d, e * e));
+          const float u = y[k], v = y[k + 1];
+          y[k]          = inv * fmaf(d, u, -e * v);
+          y[k + 1]      = inv * fmaf(e, u, d * v);
+        }
+    }
+
+    // v (NT values) <- M v for a row-major NT x NT matrix M (kernel parameter)
+    template <int NT>
+    __device__ __forceinline__ void
+    time_map(const float *M, float (&v)[NT])
+    {
+      float o[NT];
+#pragma unroll
+      for (int i = 0; i < NT; ++i)
+        {
+          float s = 0.0f;
+#pragma unroll
+          for (int j = 0; j < NT; ++j)
+            s = fmaf(M[i * NT + j], v[j], s);
+          o[i] = s;
+        }
+#pragma unroll
+      for (int i = 0; i < NT; ++i)
+        v[i] = o[i];
+    }
+
+    // Row-record apply: as the streamed apply (colour phases, records in
+    // (tile, colour, cell) order, one warp per cell, one output brick per
+    // tile), but
+    //  * each colour phase's records arrive by one bulk copy on an mbarrier;
+    //  * a record holds V by rows read as whole words, the FP32 row of mode m
+    //    ending in its eigenvalue mu_m;
+    //  * the time solves work in the eigenbasis with its two factors moved
+    //    out of the cells: the input brick is mapped by G = S^{-1} Beta^{-1}
+    //    once per tile and the tile's output by S when it is written, so a
+    //    mode's solve is the scaling of mode_scale;
+    //  * the time values of a node are added pairwise (FFMA2), the 27-term
+    //    sums split into two chains.
+    template <int DIM, int P, typename TS, int NT, int TX, int TY, int TZ>
+    __global__ void __launch_bounds__(VR_WARPS * 32, 2)
+    vanka_row_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeEig te,
+                     const unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int cpc,
+                     const float *__restrict__ src, float *__restrict__ dst, float *__restrict__ shell,
+                     const OutMode<float> om, int *__restrict__ fault)
+    {
+      using S           = TileShape<DIM, P, TX, TY, TZ>;
+      using TV          = TimeVec<NT>;
+      using RW          = RowWord<TS>;
+      using W           = typename RW::W;
+      constexpr int ND  = S::ND;
+      constexpr int NTP = TV::NTP;
+      constexpr int NA  = (NTP + 1) / 2; // accumulator pairs
+      constexpr int NR  = NT % 2;        // real eigenvalues of Beta^{-1} Alpha
+      constexpr int NC  = 1 << DIM;
+      constexpr int CPC = ((TX + 1) / 2) * ((TY + 1) / 2) * (DIM == 3 ? (TZ + 1) / 2 : 1);
+      constexpr int NW  = VR_WARPS;
+      constexpr int RS  = vk_row_stride<TS>(ND); // row stride (entries)
+      constexpr int RWD = RS / RW::PER;          // words per row
+      constexpr int RPW = 32 / S::E0;            // brick rows per warp step
+      constexpr int ROWS = NT * S::E1 * S::E2;   // rows of one input brick
+      constexpr bool MU_IN_ROW = sizeof(TS) == 4;
+      static_assert(ND <= 32, "row-record apply: at most 32 dofs per cell");
+      static_assert(S::E0 <= 32, "brick rows wider than a warp");
+      extern __shared__ __align__(16) unsigned char vk_smem[];
+      __shared__ int                             col_n[NC], col_pre[NC], col_cell[NC][CPC];
+      __shared__ __align__(8) unsigned long long bars[VR_STAGES];
+      const int       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const int       lrow = lane / S::E0, lx = lane - lrow * S::E0;
+      const long long stage_bytes = (long long)cpc * rec_bytes;
+      float          *bin0 = reinterpret_cast<float *>(vk_smem + VR_STAGES * stage_bytes);
+      float          *bout = bin0 + 2 * S::NB * NTP;
+      float          *wb   = bout + S::NB * NTP + warp * ND * NTP;
+      const long long tcr  = (long long)tl.T[0] * tl.T[1] * tl.T[2];
+      const int       my_tiles = int(blockIdx.x) < tl.n_tiles ? int((tl.n_tiles - 1 - blockIdx.x) / gridDim.x) + 1 : 0;
+      const int       phases   = my_tiles * NC;
+
+      if (threadIdx.x < NC)
+        {
+          const int col = threadIdx.x;
+          int       cnt[3], n = 1, pre = 0;
+          for (int c = 0; c <= col; ++c)
+            {
+              int nc = 1;
+#pragma unroll
+              for (int d = 0; d < 3; ++d)
+                {
+                  const int o = (c >> d) & 1;
+                  cnt[d]      = d < DIM ? (tl.T[d] - o + 1) / 2 : (o ? 0 : 1);
+                  nc *= cnt[d];
+                }
+              if (c < col)
+                pre += nc;
+              else
+                n = nc;
+            }
+          col_n[col]   = n;
+          col_pre[col] = pre;
+          for (int idx = 0; idx < n && idx < CPC; ++idx)
+            {
+              const int ix = idx % cnt[0], iy = (idx / cnt[0]) % cnt[1], iz = idx / (cnt[0] * cnt[1]);
+              const int cx = 2 * ix + (col & 1), cy = 2 * iy + ((col >> 1) & 1), cz = 2 * iz + ((col >> 2) & 1);
+              col_cell[col][idx] = cx | (cy << 8) | (cz << 16);
+            }
+        }
+      if (threadIdx.x == 0)
+        {
+          for (int st = 0; st < VR_STAGES; ++st)
+            mbar_init(smem_u32(&bars[st]), 1);
+          asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+      for (int idx = threadIdx.x; idx < S::NB * NTP; idx += blockDim.x)
+        bout[idx] = 0.0f;
+      __syncthreads();
+
+      // phase k: the colour phase's records by one bulk copy (thread 0) and,
+      // for a tile's first colour, the tile's input brick (cp.async group)
+      auto issue = [&](int k) {
+        if (k < phases)
+          {
+            const int tile = blockIdx.x + (k / NC) * gridDim.x;
+            const int col  = k % NC;
+            if (threadIdx.x == 0)
+              {
+                const unsigned bar   = smem_u32(&bars[k % VR_STAGES]);
+                const unsigned bytes = unsigned(col_n[col]) * unsigned(rec_bytes);
+                if (bytes > 0)
+                  {
+                    fence_proxy_async_smem();
+                    mbar_expect_tx(bar, bytes);
+                    bulk_copy_g2s(smem_u32(vk_smem + (k % VR_STAGES) * stage_bytes),
+                                  rec + (tile * tcr + col_pre[col]) * rec_bytes, bytes, bar);
+                  }
+                else
+                  mbar_arrive(bar);
+              }
+            if (col == 0)
+              {
+                const TileGeo tg  = tile_geo<DIM, P>(m, tl, tile);
+                float        *bi  = bin0 + ((k / NC) & 1) * S::NB * NTP;
+                const int     gx  = tg.c0[0] * P + lx;
+                const bool    okx = lx < tg.e[0] && gx > 0 && gx < m.nn[0] - 1;
+                for (int rb = warp * RPW; rb < ROWS; rb += NW * RPW)
+                  {
+                    const int row = rb + lrow;
+                    if (lrow >= RPW || row >= ROWS)
+                      continue;
+                    const int i = row / (S::E1 * S::E2), rem = row - i * (S::E1 * S::E2);
+                    const int bz = rem / S::E1, by = rem - bz * S::E1;
+                    const int gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
+                    bool      ok = okx && by < tg.e[1] && bz < tg.e[2] && gy > 0 && gy < m.nn[1] - 1;
+                    if (DIM == 3)
+                      ok = ok && gz > 0 && gz < m.nn[2] - 1;
+                    const float *gp = ok ? src + i * m.N + gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz) : src;
+                    cp_async_small<4>(bi + ((bz * S::E1 + by) * S::E0 + lx) * NTP + i, gp, ok);
+                  }
+              }
+          }
+        cp_async_commit();
+      };
+
+#pragma unroll
+      for (int k = 0; k < VR_STAGES - 1; ++k)
+        issue(k);
+
+      TileGeo tg{};
+      int     k = 0;
+      for (; k < phases; ++k)
+        {
+          const bool arrived = mbar_wait(smem_u32(&bars[k % VR_STAGES]), unsigned(k / VR_STAGES) & 1u);
+          cp_async_wait<VR_STAGES - 2>();
+          // phase k's records and brick visible; phase k-1 done (its stage free, its output adds made)
+          if (__syncthreads_or(!arrived))
+            break;
+          issue(k + VR_STAGES - 1);
+
+          const int tile = blockIdx.x + (k / NC) * gridDim.x;
+          const int col  = k % NC;
+          float    *bi   = bin0 + ((k / NC) & 1) * S::NB * NTP;
+          if (col == 0)
+            {
+              tg = tile_geo<DIM, P>(m, tl, tile);
+              // the tile's input in the eigenbasis: x <- G x per node
+              for (int nd = threadIdx.x; nd < S::NB; nd += blockDim.x)
+                {
+                  float v[NT];
+                  TV::load(bi + nd * NTP, v);
+                  time_map<NT>(te.G, v);
+                  TV::store(bi + nd * NTP, v);
+                }
+              __syncthreads();
+            }
+          const int            n   = col_n[col];
+          const unsigned char *stg = vk_smem + (k % VR_STAGES) * stage_bytes;
+          for (int idx = warp; idx < n; idx += NW)
+            {
+              const int cl = col_cell[col][idx];
+              const int cx = cl & 255, cy = (cl >> 8) & 255, cz = cl >> 16;
+              if (cx >= tg.tc[0] || cy >= tg.tc[1] || cz >= tg.tc[2])
+                continue;
+              const unsigned char *r     = stg + idx * rec_bytes;
+              const TS            *V     = reinterpret_cast<const TS *>(r);
+              const int            bbase = cx * P + S::E0 * (cy * P + S::E1 * (cz * P));
+
+              // pass 1 (lane = mode): y = V x, then the mode's time solve
+              {
+                const int mm  = lane < ND ? lane : ND - 1;
+                const W  *row = reinterpret_cast<const W *>(V + mm * RS);
+                W         vw[RWD];
+#pragma unroll
+                for (int q = 0; q < RWD; ++q)
+                  vw[q] = row[q];
+                float2 ya[NA], yb[NA];
+#pragma unroll
+                for (int q = 0; q < NA; ++q)
+                  ya[q] = yb[q] = make_float2(0.0f, 0.0f);
+#pragma unroll
+                for (int a = 0; a < ND; ++a)
+                  {
+                    const float  v = RW::get(vw[a / RW::PER], a % RW::PER);
+                    const float *x = bi + (bbase + S::offset(a)) * NTP;
+                    if (a & 1)
+                      acc_time<NTP>(yb, v, x);
+                    else
+                      acc_time<NTP>(ya, v, x);
+                  }
+                float mu;
+                if constexpr (MU_IN_ROW)
+                  mu = RW::get(vw[ND / RW::PER], ND % RW::PER);
+                else
+                  mu = reinterpret_cast<const float *>(r + mu_off)[mm];
+                float y[NT];
+#pragma unroll
+                for (int i = 0; i < NT; ++i)
+                  y[i] = (i & 1) ? ya[i / 2].y + yb[i / 2].y : ya[i / 2].x + yb[i / 2].x;
+                mode_scale<NT, NR>(te, mu, y);
+                if (lane < ND)
+                  TV::store(wb + lane * NTP, y);
+              }
+              __syncwarp();
+              // pass 2 (lane = dof): out = V^T w, added into the output brick
+              {
+                const int a = lane < ND ? lane : ND - 1;
+                float2    oa[NA], ob[NA];
+#pragma unroll
+                for (int q = 0; q < NA; ++q)
+                  oa[q] = ob[q] = make_float2(0.0f, 0.0f);
+#pragma unroll 9
+                for (int mm = 0; mm < ND; ++mm)
+                  {
+                    const float v = load_s(V + mm * RS + a);
+                    if (mm & 1)
+                      acc_time<NTP>(ob, v, wb + mm * NTP);
+                    else
+                      acc_time<NTP>(oa, v, wb + mm * NTP);
+                  }
+                if (lane < ND)
+                  {
+                    float *o = bout + (bbase + S::offset(a)) * NTP;
+                    float  cur[NT];
+                    TV::load(o, cur);
+#pragma unroll
+                    for (int i = 0; i < NT; ++i)
+                      cur[i] += (i & 1) ? oa[i / 2].y + ob[i / 2].y : oa[i / 2].x + ob[i / 2].x;
+                    TV::store(o, cur);
+                  }
+              }
+              __syncwarp();
+            }
+          if (col == NC - 1)
+            {
+              __syncthreads();
+              // the tile's output (back from the eigenbasis: o <- S o), as in
+              // the streamed apply
+              const int  gx  = tg.c0[0] * P + lx;
+              const int  vx  = (gx % P == 0) ? 2 : 1;
+              const bool inx = lx > 0 && lx < tg.e[0] - 1;
+              for (int rb = warp * RPW; rb < S::E1 * S::E2; rb += NW * RPW)
+                {
+                  const int row = rb + lrow;
+                  if (lrow >= RPW || row >= S::E1 * S::E2 || lx >= tg.e[0])
+                    continue;
+                  const int bz = row / S::E1, by = row - bz * S::E1;
+                  if (by >= tg.e[1] || bz >= tg.e[2])
+                    continue;
+                  bool inte = inx && by > 0 && by < tg.e[1] - 1;
+                  if (DIM == 3)
+                    inte = inte && bz > 0 && bz < tg.e[2] - 1;
+                  const int gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
+                  int       v  = vx * ((gy % P == 0) ? 2 : 1);
+                  if (DIM == 3)
+                    v *= (gz % P == 0) ? 2 : 1;
+                  const float w = v == 1 ? 1.0f : (v == 2 ? 0.5f : (v == 4 ? 0.25f : 0.125f));
+                  float       o[NT];
+                  TV::load(bout + ((bz * S::E1 + by) * S::E0 + lx) * NTP, o);
+                  time_map<NT>(te.S, o);
+                  long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+                  if (inte)
+#pragma unroll
+                    for (int jt = 0; jt < NT; ++jt, gi += m.N)
+                      om.write(dst, gi, o[jt] * w);
+                  else if (tl.n_tiles == 1)
+#pragma unroll
+                    for (int jt = 0; jt < NT; ++jt, gi += m.N)
+                      om.write_constrained(dst, gi);
+                  else
+                    {
+                      float *sj = shell + (long long)tile * NT * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz);
+#pragma unroll
+                      for (int jt = 0; jt < NT; ++jt, sj += tl.tile_stride)
+                        *sj = o[jt];
+                    }
+                }
+              __syncthreads();
+              for (int idx = threadIdx.x; idx < S::NB * NTP; idx += blockDim.x)
+                bout[idx] = 0.0f;
+            }
+        }
+      if (k < phases)
+        {
+          // a record copy did not arrive in time: flag it, wait (bounded) for
+          // the copies this CTA issued and return
+          if (threadIdx.x == 0)
+            {
+              atomicExch(fault, 1);
+              const int last = min(phases, k + VR_STAGES - 1);
+              for (int j = k; j < last; ++j)
+                mbar_wait(smem_u32(&bars[j % VR_STAGES]), unsigned(j / VR_STAGES) & 1u);
+            }
+          __syncthreads();
+        }
+      cp_async_wait<0>();
+    }
+
     // compile-time tile shapes of the Vanka apply (main and fallback)
     template <int DIM, int P, bool BIG>
     struct VkShape
@@ -715,10 +1183,42 @@ namespace stmg
         launch_plane_fixup<DIM, float, true>(m, tl, vk.nt, reinterpret_cast<float *>(vk.shell.ptr), dst, om, s);
     }
 
+    template <int DIM, int P, typename TS, int NT, bool BIG>
+    void
+    launch_row(const Vanka &vk, const float *src, float *dst, const OutMode<float> &om, cudaStream_t s)
+    {
+      using Sh = VkShape<DIM, P, BIG>;
+      if constexpr (Tens<P + 1, DIM>::ND <= 32)
+        {
+          const MeshView   &m    = vk.mesh->v;
+          const Tiling     &tl   = vk.tiling;
+          const std::size_t smem = vk.smem_bytes(vk.shape);
+          auto              kern = vanka_row_kernel<DIM, P, TS, NT, Sh::TX, Sh::TY, Sh::TZ>;
+          const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), VR_WARPS * 32, smem, tl.n_tiles);
+          kern<<<grid, VR_WARPS * 32, smem, s>>>(m, tl, vk.teig, vk.V.ptr, vk.rec_bytes, vk.mu_off, vk.colour_cells, src,
+                                                 dst, reinterpret_cast<float *>(vk.shell.ptr), om,
+                                                 vanka_fault_flag_device());
+          count_launch();
+          STMG_CUDA(cudaGetLastError());
+          if (tl.n_tiles > 1)
+            launch_plane_fixup<DIM, float, true>(m, tl, vk.nt, reinterpret_cast<float *>(vk.shell.ptr), dst, om, s);
+        }
+      else
+        throw Error(STMG_ERR_UNSUPPORTED, "vanka: row records need at most 32 dofs per cell");
+    }
+
     template <int DIM, int P, typename TS, int NT>
     void
     launch_stream_nt(const Vanka &vk, const float *src, float *dst, const OutMode<float> &om, cudaStream_t s)
     {
+      if (vk.rowrec)
+        {
+          if (vk.big)
+            launch_row<DIM, P, TS, NT, true>(vk, src, dst, om, s);
+          else
+            launch_row<DIM, P, TS, NT, false>(vk, src, dst, om, s);
+          return;
+        }
       if (vk.big)
         launch_stream<DIM, P, TS, NT, true>(vk, src, dst, om, s);
       else
