@@ -504,53 +504,99 @@ def run_config(args):
     return 0
 
 
+def smoothed_field(n, seed, sigma_cells=1.0):
+    """White noise N(0, 1) on the n^3 cells, smoothed by a Gaussian of
+    sigma_cells cells (scipy.ndimage.gaussian_filter, reflecting edges) and
+    scaled back to unit standard deviation."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    w = gaussian_filter(rng.standard_normal((n, n, n)), sigma=sigma_cells, mode="reflect")
+    return (w / w.std()).reshape(-1)
+
+
 def run_adjoint(args):
     """--adjoint: the adjoint-gradient configuration: heat, 32^3 Q2 cells,
-    dG(1), 16 slabs of dt = 1/16, per-cell log-coefficient ~ N(0, 1),
-    observations from a forward FP64 solve with a perturbed field plus 1e-3
-    relative noise; the misfit gradient with checkpoints every 4 slabs
-    (FP64 multigrid, 1e-12), timed, and checked against central finite
-    differences on --fd random unit directions (h = 1e-4)."""
+    dG(1), 16 slabs of dt = 1/16, f = 1. The true log-coefficient is
+    Gaussian-smoothed white noise (sigma = 1 cell, unit standard deviation,
+    seeded); the observations are a forward FP64 solve with the true field
+    plus 1e-3 relative Gaussian noise; the gradient of the misfit is taken at
+    the initial guess theta = 0 with checkpoints every 4 slabs (FP64
+    multigrid, 1e-12), through the torch.autograd.Function wrapper, timed,
+    and checked against central finite differences of forward solves on
+    --fd random unit directions (h = 1e-4). The same construction on 8^3
+    cells is checked against central differences of the oracle's FP64 solves
+    (--fd-oracle directions)."""
     import torch
     import stmg
-    n, S = 32, 16
-    rng = np.random.default_rng(SEED)
-    theta = rng.normal(0.0, 1.0, n ** 3)
-    f = np.ones((2 * n + 1) ** 3)
-    kw = dict(dim=3, refine=5, degree=2, time_degree=1, time_type=stmg.DG, problem=stmg.HEAT, n_steps=1, tau=1 / 16,
-              fe_degree_min=0, n_steps_min=1, rhs_mode=1, f_nodal=f, tol=1e-12, abs_tol=1e-300, mg_dtype=stmg.F64)
+    from stmg.adjoint import misfit, misfit_value
+    import oracle_py as orc
 
-    def solver(th):
-        return stmg.Solver(fine_coeff=np.exp(th), **kw)
+    def setup(n, S, seed):
+        rng = np.random.default_rng(seed)
+        truth = smoothed_field(n, seed)
+        f = np.ones((2 * n + 1) ** 3)
+        kw = dict(dim=3, refine=int(np.log2(n)), degree=2, time_degree=1, time_type=stmg.DG, problem=stmg.HEAT,
+                  n_steps=1, tau=1 / 16, fe_degree_min=0, n_steps_min=1, rhs_mode=1, f_nodal=f, tol=1e-12,
+                  abs_tol=1e-300, mg_dtype=stmg.F64)
 
-    def forward(th):
-        sv, out = solver(th), []
+        def make(kappa):
+            return stmg.Solver(fine_coeff=kappa, **kw)
+
+        clean = []
+        sv = make(np.exp(truth))
         for _ in range(S):
             sv.run(1)
-            u, _ = sv.solution(want_v=False)
-            out.append(u)
-        return np.array(out)
+            clean.append(sv.solution(want_v=False)[0])
+        clean = np.array(clean)
+        obs = clean * (1 + 1e-3 * rng.standard_normal(clean.shape))
+        return rng, truth, f, make, obs
 
-    clean = forward(0.9 * theta)
-    obs = clean * (1 + 1e-3 * rng.standard_normal(clean.shape))
-    s = solver(theta)
+    n, S = 32, 16
+    rng, truth, f, make, obs = setup(n, S, SEED)
+    theta = torch.zeros(n ** 3, dtype=torch.float64, requires_grad=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    J, g, itf, ita = s.gradient(obs, checkpoint_every=4)
+    J = misfit(theta, make, obs, 4)
+    J.backward()
     torch.cuda.synchronize()
     t = time.perf_counter() - t0
+    g = theta.grad.numpy()
     checks = []
+    h = 1e-4
     for _ in range(args.fd):
-        d = rng.standard_normal(theta.size)
+        d = rng.standard_normal(theta.numel())
         d /= np.linalg.norm(d)
-        h = 1e-4
-        Jp = 0.5 * float(np.sum((forward(theta + h * d) - obs) ** 2))
-        Jm = 0.5 * float(np.sum((forward(theta - h * d) - obs) ** 2))
-        fd = (Jp - Jm) / (2 * h)
+        fd = (misfit_value(h * d, make, obs) - misfit_value(-h * d, make, obs)) / (2 * h)
         checks.append(dict(gd=float(g @ d), fd=fd, rel=abs(float(g @ d) - fd) / max(abs(fd), 1e-300)))
-    print(json.dumps(dict(workload="heat3d-32^3-Q2-dG1-16slabs-adjoint", misfit=J, gradient_seconds=t,
-                          fgmres_forward=int(itf.sum()), fgmres_adjoint=int(ita.sum()), checkpoint_every=4,
-                          fd_checks=checks)), flush=True)
+
+    # the same construction on 8^3 cells: GPU gradient against central
+    # differences of the oracle's FP64 solves
+    n8 = 8
+    rng8, truth8, f8, make8, obs8 = setup(n8, S, SEED + 1)
+    th8 = torch.zeros(n8 ** 3, dtype=torch.float64, requires_grad=True)
+    J8 = misfit(th8, make8, obs8, 4)
+    J8.backward()
+    g8 = th8.grad.numpy()
+
+    def oracle_misfit(th):
+        r = orc.run(dim=3, refine=3, p=2, r=1, ttype=orc.DG, problem=orc.HEAT, n_steps=1, tau=1 / 16, n_slabs=S,
+                    fe_degree_min=0, n_steps_min=1, mg_float=False, tol=1e-13, abs_tol=1e-300, rhs_mode=1, f_nodal=f8,
+                    fine_coeff=np.exp(th), compute_errors=False, keep_all=True)
+        return 0.5 * float(np.sum((r["u_all"] - obs8) ** 2))
+
+    ochecks = []
+    for _ in range(args.fd_oracle):
+        d = rng8.standard_normal(n8 ** 3)
+        d /= np.linalg.norm(d)
+        fd = (oracle_misfit(h * d) - oracle_misfit(-h * d)) / (2 * h)
+        ochecks.append(dict(gd=float(g8 @ d), fd_oracle=fd, rel=abs(float(g8 @ d) - fd) / max(abs(fd), 1e-300)))
+    print(json.dumps(dict(workload="heat3d-32^3-Q2-dG1-16slabs-adjoint", misfit=float(J), gradient_seconds=t,
+                          parameters=int(theta.numel()), initial_guess="theta = 0",
+                          true_field="Gaussian-smoothed white noise, sigma 1 cell, unit std",
+                          checkpoint_every=4, fd_h=h, fd_checks=checks,
+                          max_fd_rel=max(c["rel"] for c in checks) if checks else None,
+                          oracle_check=dict(workload="heat3d-8^3-Q2-dG1-16slabs", misfit=float(J8),
+                                            checks=ochecks))), flush=True)
     return 0
 
 
@@ -572,7 +618,9 @@ def main():
     ap.add_argument("--adjoint", action="store_true", help="time the adjoint gradient configuration")
     ap.add_argument("--config", choices=["c1", "c2", "c3"], default=None,
                     help="time one of the other configurations (not the main metric line)")
-    ap.add_argument("--fd", type=int, default=2, help="finite-difference directions checked with --adjoint")
+    ap.add_argument("--fd", type=int, default=8, help="finite-difference directions checked with --adjoint")
+    ap.add_argument("--fd-oracle", type=int, default=2,
+                    help="directions checked against the oracle's FP64 solves with --adjoint (8^3 cells)")
     args = ap.parse_args()
     if args.adjoint:
         return run_adjoint(args)

@@ -62,6 +62,26 @@ def build(jobs=8, verbose_ptxas=False):
     return LIB
 
 
+CPP_TESTS = [(os.path.join(REPO, "tests", "cpp", "shim_test.cc"), os.path.join(REPO, "tests", "cpp", "build", "shim_test"))]
+
+
+def build_cpp_tests():
+    """Host C++ programs of tests/cpp (the drop-in classes of
+    include/stmg_dealii.hpp over the C ABI), linked against the in-tree
+    library with a relative run path so they run wherever the tree is."""
+    cuda = os.path.dirname(os.path.dirname(NVCC))
+    for src, exe in CPP_TESTS:
+        os.makedirs(os.path.dirname(exe), exist_ok=True)
+        deps = [src, LIB, os.path.join(REPO, "include", "stmg_dealii.hpp"), os.path.join(REPO, "include", "stmg.h")]
+        if os.path.exists(exe) and os.path.getmtime(exe) >= max(os.path.getmtime(d) for d in deps):
+            continue
+        cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(REPO, "include"), "-I",
+               os.path.join(cuda, "include"), src, "-L", HERE, "-lstmg_cuda", "-L", os.path.join(cuda, "lib64"),
+               "-lcudart", "-Wl,-rpath,$ORIGIN/../../../dealii-stfem_b200", "-o", exe]
+        subprocess.run(cmd, check=True)
+
+
 if __name__ == "__main__":
     jobs = int(sys.argv[sys.argv.index("-j") + 1]) if "-j" in sys.argv else 8
     print(build(jobs, verbose_ptxas="--ptxas-v" in sys.argv))
+    build_cpp_tests()

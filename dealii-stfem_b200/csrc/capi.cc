@@ -184,6 +184,13 @@ extern "C"
   }
 
   int
+  stmg_block_permute(int n_blocks, long long n, const long long *perm, int scatter, const void *src, void *dst,
+                     int dtype, void *stream)
+  {
+    return guard([&] { block_permute(n_blocks, n, perm, scatter, src, dst, dtype, static_cast<cudaStream_t>(stream)); });
+  }
+
+  int
   stmg_mesh_create(int dim, const int *n_cells, int degree, const double *lo, const double *hi, const double *vertices,
                    int coeff_mode, const double *coeff, stmg_mesh_t *mesh)
   {
@@ -257,6 +264,7 @@ extern "C"
   stmg_op_vmult(stmg_op_t op, void *dst, const void *src, void *stream)
   {
     return guard([&] {
+      NvtxScope range("vmult");
       STMG_REQUIRE(op && op->op, STMG_ERR_HANDLE, "op_vmult: null handle");
       op->op->apply(false, src, dst, false, static_cast<cudaStream_t>(stream));
     });
@@ -274,9 +282,19 @@ extern "C"
   }
 
   int
+  stmg_op_diagonal(stmg_op_t op, int inverse, void *dst, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(op && op->op, STMG_ERR_HANDLE, "op_diagonal: null handle");
+      op->op->diagonal(inverse != 0, dst, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
   stmg_op_Tvmult(stmg_op_t op, void *dst, const void *src, void *stream)
   {
     return guard([&] {
+      NvtxScope range("Tvmult");
       STMG_REQUIRE(op && op->op, STMG_ERR_HANDLE, "op_Tvmult: null handle");
       op->op->apply(true, src, dst, false, static_cast<cudaStream_t>(stream));
     });
@@ -286,6 +304,7 @@ extern "C"
   stmg_op_vmult_add(stmg_op_t op, void *dst, const void *src, void *stream)
   {
     return guard([&] {
+      NvtxScope range("vmult");
       STMG_REQUIRE(op && op->op, STMG_ERR_HANDLE, "op_vmult_add: null handle");
       op->op->apply(false, src, dst, true, static_cast<cudaStream_t>(stream));
     });
@@ -317,8 +336,25 @@ extern "C"
   stmg_vanka_vmult(stmg_vanka_t vanka, void *dst, const void *src, void *stream)
   {
     return guard([&] {
+      NvtxScope range("vanka");
       STMG_REQUIRE(vanka && vanka->vk, STMG_ERR_HANDLE, "vanka_vmult: null handle");
       vanka->vk->apply(src, dst, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_relax_step(stmg_vanka_t vanka, stmg_op_t op, double omega, void *x, const void *b, void *tmp, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(vanka && vanka->vk && op && op->op, STMG_ERR_HANDLE, "relax_step: null handle");
+      STMG_REQUIRE(x && b && tmp, STMG_ERR_ARG, "relax_step: null vector");
+      const Vanka      &vk = *vanka->vk;
+      const StOperator &A  = *op->op;
+      STMG_REQUIRE(A.mesh == vk.mesh && A.nt_in == vk.nt && A.nt_out == vk.nt && A.dtype == vk.compute, STMG_ERR_SHAPE,
+                   "relax_step: operator and smoother differ in mesh, time dofs or type");
+      const cudaStream_t s = static_cast<cudaStream_t>(stream);
+      A.apply_ex(false, x, tmp, -1.0, 0.0, b, s); // tmp = b - A x
+      vk.apply_ex(tmp, x, omega, 1.0, s);         // x += omega P tmp
     });
   }
 
@@ -493,6 +529,31 @@ extern "C"
       STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_set_source: null handle");
       STMG_REQUIRE(f_nodal, STMG_ERR_ARG, "solver_set_source: null source");
       solver->s->set_source(f_nodal);
+    });
+  }
+
+  int
+  stmg_solver_point_values(stmg_solver_t solver, int n_points, const double *points, int samples_per_step,
+                           double *times, double *values, void *stream)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_point_values: null handle");
+      const int r       = solver->s->cfg.time_degree;
+      const int samples = samples_per_step > 0 ? samples_per_step : (r + 1) * (r + 1);
+      solver->s->point_values(n_points, points, samples, times, values, static_cast<cudaStream_t>(stream));
+    });
+  }
+
+  int
+  stmg_solver_set_control(stmg_solver_t solver, double tol, double abs_tol, int max_iter)
+  {
+    return guard([&] {
+      STMG_REQUIRE(solver && solver->s, STMG_ERR_HANDLE, "solver_set_control: null handle");
+      STMG_REQUIRE(tol >= 0 && abs_tol >= 0 && max_iter >= 1, STMG_ERR_ARG,
+                   "solver_set_control: tolerances >= 0 and max_iter >= 1");
+      solver->s->cfg.tol      = tol;
+      solver->s->cfg.abs_tol  = abs_tol;
+      solver->s->cfg.max_iter = max_iter;
     });
   }
 

@@ -367,22 +367,24 @@ namespace stmg
       rm[e]             = T(cm[r + c * n]);
     }
 
-    // y = C x, one warp per row, fixed reduction order
+    // y = C x with C in FP64 and FP64 accumulation whatever the vectors'
+    // type (the coarse-grid map stays FP64 inside an FP32 V-cycle); one warp
+    // per row, fixed reduction order
     template <typename T>
     __global__ void
-    dense_matvec_kernel(int n, const T *__restrict__ C, const T *__restrict__ x, T *__restrict__ y)
+    dense_matvec_kernel(int n, const double *__restrict__ C, const T *__restrict__ x, T *__restrict__ y)
     {
       const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
       if (row >= n)
         return;
-      T acc = T(0);
+      double acc = 0.0;
       for (int j = lane; j < n; j += 32)
-        acc += C[(long long)row * n + j] * x[j];
+        acc += C[(long long)row * n + j] * double(x[j]);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1)
         acc += __shfl_xor_sync(0xffffffffu, acc, o);
       if (lane == 0)
-        y[row] = acc;
+        y[row] = T(acc);
     }
 
     // ------------------------------------------------- right-hand side
@@ -747,12 +749,9 @@ namespace stmg
         STMG_CUDA(cudaStreamSynchronize(s));
       }
     const long long n = levels[t].size();
-    tail_mat.alloc(std::size_t(n * n) * (dtype == STMG_F64 ? 8 : 4));
+    tail_mat.alloc(std::size_t(n * n) * 8);
     const unsigned nb = unsigned((n * n + 255) / 256);
-    if (dtype == STMG_F64)
-      to_rowmajor_kernel<double><<<nb, 256, 0, s>>>(n, C.m.ptr, reinterpret_cast<double *>(tail_mat.ptr));
-    else
-      to_rowmajor_kernel<float><<<nb, 256, 0, s>>>(n, C.m.ptr, reinterpret_cast<float *>(tail_mat.ptr));
+    to_rowmajor_kernel<double><<<nb, 256, 0, s>>>(n, C.m.ptr, reinterpret_cast<double *>(tail_mat.ptr));
     STMG_CUDA(cudaGetLastError());
     STMG_CUDA(cudaStreamSynchronize(s));
     tail = t;
@@ -811,7 +810,8 @@ namespace stmg
     if (l == tail)
       {
         const long long n = lv.size();
-        dense_matvec_kernel<T><<<unsigned((n + 7) / 8), 256, 0, s>>>(int(n), as<T>(tail_mat), as<T>(lv.def), as<T>(lv.sol));
+        dense_matvec_kernel<T><<<unsigned((n + 7) / 8), 256, 0, s>>>(int(n), as<double>(tail_mat), as<T>(lv.def),
+                                                                     as<T>(lv.sol));
         count_launch();
         STMG_CUDA(cudaGetLastError());
         return;
@@ -878,6 +878,7 @@ namespace stmg
     // scale * src and its result is multiplied by 1 / scale, both exact, so
     // dst is the same to the last bit while the cycle's vectors keep a
     // moderate size in its own precision.
+    NvtxScope       range("gmg");
     Level          &top = levels.back();
     const long long n   = top.size();
     if (dtype == STMG_F64)
@@ -1236,7 +1237,10 @@ namespace stmg
   int
   SlabSolver::solve(double *xv, const double *b, cudaStream_t s)
   {
-    auto Aop = [&](double *dst, const double *src) { A64->apply(false, src, dst, false, s); };
+    auto Aop = [&](double *dst, const double *src) {
+      NvtxScope r("vmult");
+      A64->apply(false, src, dst, false, s);
+    };
     auto Pop = [&](double *dst, const double *src, double scale) { gmg->vmult(dst, src, s, scale); };
     return gmres->solve(Aop, Pop, xv, b, cfg.abs_tol, cfg.tol, cfg.max_iter, s);
   }
@@ -1249,6 +1253,7 @@ namespace stmg
     const std::vector<double> tq   = tfe::basis_points(type, cfg.time_degree);
     for (int slab = 0; slab < n_slabs; ++slab)
       {
+        NvtxScope step_range("step");
         STMG_CUDA(cudaMemcpyAsync(prev_x.ptr, x.ptr + (nb - 1) * N, N * 8, cudaMemcpyDeviceToDevice, s));
         if (cfg.problem == 2)
           STMG_CUDA(cudaMemcpyAsync(prev_v.ptr, v.ptr + (nb - 1) * N, N * 8, cudaMemcpyDeviceToDevice, s));
@@ -1441,7 +1446,10 @@ namespace stmg
     DevBuf<double> x_end(n);
     STMG_CUDA(cudaMemcpyAsync(x_end.ptr, x.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
     const double t_end = time;
-    auto         AT    = [&](double *dst, const double *src) { A64->apply(true, src, dst, false, s); };
+    auto         AT    = [&](double *dst, const double *src) {
+      NvtxScope r("Tvmult");
+      A64->apply(true, src, dst, false, s);
+    };
     auto         PT    = [&](double *dst, const double *src, double scale) { gmgT->vmult(dst, src, s, scale); };
     bool         have_next = false;
     for (int seg = nseg - 1; seg >= 0; --seg)

@@ -66,7 +66,8 @@ namespace stmg
     // Levels 0..tail (tail >= 0) run as one dense matrix C: with fixed
     // relaxation weights and sweep counts the V-cycle from level `tail` down
     // is the linear map sol = C def, composed once in FP64 from dense copies
-    // of the levels' operators, smoothers and transfers. -1: none.
+    // of the levels' operators, smoothers and transfers, and applied in FP64
+    // (the coarse-grid solve stays FP64 in the FP32 V-cycle). -1: none.
     int tail = -1;
     static constexpr long long DENSE_TAIL_MAX = 4096; // entries per level vector
 
@@ -91,7 +92,7 @@ namespace stmg
     cudaGraphExec_t graph     = nullptr;
     cudaStream_t    cap       = nullptr;
     long long       graph_nodes = 0;
-    DevBuf<unsigned char> tail_mat; // n x n row-major in the V-cycle's type
+    DevBuf<unsigned char> tail_mat; // n x n row-major, FP64 (applied in FP64 in either V-cycle type)
   };
 
   // FGMRES(restart) with CGS2 orthogonalisation on device vectors.
@@ -143,6 +144,13 @@ namespace stmg
     // and recomputed segment by segment. Leaves the state after the last slab.
     double gradient(int n_slabs, const double *obs, int checkpoint_every, double *grad, int *its_fwd,
                     int *its_adj, cudaStream_t s);
+
+    // Point functionals of the last slab (tests/tp_01.cc:451-619): u at the
+    // n_pts points (host, n_pts x dim) for each time node, mapped to
+    // `samples` equidistant times per step by the Lagrange time basis;
+    // values: host, (n_steps samples) x n_pts; times (may be null): the
+    // sample times
+    void point_values(int n_pts, const double *pts, int samples, double *times, double *values, cudaStream_t s);
 
     SolverConfig                        cfg;
     std::vector<std::unique_ptr<Mesh>>  meshes; // coarsest first

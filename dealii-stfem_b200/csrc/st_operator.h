@@ -58,6 +58,10 @@ namespace stmg
         return qtab32;
     }
     std::size_t smem_bytes(const int *shape, int nt_in, int nt_out, std::size_t elem) const;
+    // SystemMatrix::get_matrix_diagonal (inverse = false) or
+    // get_matrix_diagonal_inverse (operators.h:188-215) into dst (nt blocks,
+    // the operator's type); the spatial diagonals are computed on first use
+    void diagonal(bool inverse, void *dst, cudaStream_t s) const;
 
   private:
     Tiling choose_tiling(int nt_in, int nt_out, bool &big, int *shape) const;
@@ -69,7 +73,11 @@ namespace stmg
     QTab<double>     qtab64;
     QTab<float>      qtab32;
     DevBuf<unsigned char> shell; // tile face slots (scratch, allocated at creation)
+    mutable DevBuf<double> diag_K, diag_M; // spatial diagonals (first diagonal() call)
   };
+
+  // diagonals of K and M of a mesh (constrained rows 1), FP64, by probing
+  void spatial_diagonals(Mesh *mesh, double *dK, double *dM, cudaStream_t s);
 
   // dst = (A (x) K + B (x) M) src on the uniform box [lo, hi] with n_cells
   // cells, allocating no device memory (face slots in a fixed device array

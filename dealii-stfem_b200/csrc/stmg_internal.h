@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <memory>
@@ -11,6 +12,8 @@
 #include <vector>
 
 #include "../../include/stmg.h"
+
+#include <nvtx3/nvToolsExt.h>
 
 namespace stmg
 {
@@ -28,6 +31,18 @@ namespace stmg
   };
 
   void set_last_error(const std::string &m);
+
+  // NVTX range over a scope, named like the reference's TimerOutput sections
+  // ("vmult", "Tvmult", "vanka", "gmg", "step": operators.h:97,127,158,
+  // gmg.h:479,850, tp_01.cc:632), so a profiler's timeline shows the same
+  // breakdown; costs nothing without a profiler attached.
+  struct NvtxScope
+  {
+    explicit NvtxScope(const char *name) { nvtxRangePushA(name); }
+    ~NvtxScope() { nvtxRangePop(); }
+    NvtxScope(const NvtxScope &)            = delete;
+    NvtxScope &operator=(const NvtxScope &) = delete;
+  };
 
   // Number of kernels this library has launched (diagnostic counter).
   void      count_launch();
@@ -190,6 +205,10 @@ namespace stmg
   // (occupancy with the given block size and dynamic shared memory), at most
   // `work` CTAs. Also raises the kernel's dynamic shared-memory limit.
   unsigned persistent_grid(const void *kernel, int block, std::size_t smem, long long work);
+  // dst[b][i] = src[b][perm[i]] (scatter = 0) or dst[b][perm[i]] = src[b][i]
+  // (scatter = 1) for n_blocks blocks of n entries; perm on the device
+  void block_permute(int n_blocks, long long n, const long long *perm, int scatter, const void *src, void *dst,
+                     int dtype, cudaStream_t s);
   int      sm_count();
 
   // Time coupling matrices of an operator (kernel parameter).

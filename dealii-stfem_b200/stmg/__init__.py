@@ -159,6 +159,10 @@ class Operator:
     def vmult_add(self, dst, src, stream=None):
         check(lib().stmg_op_vmult_add(self.h, _dev(dst), _dev(src), _stream(stream)))
 
+    def diagonal(self, dst, inverse=False, stream=None):
+        """get_matrix_diagonal / get_matrix_diagonal_inverse into dst."""
+        check(lib().stmg_op_diagonal(self.h, int(inverse), _dev(dst), _stream(stream)))
+
 
 class Vanka:
     """stmg_vanka_t: cell-patch space-time Vanka smoother of one level."""
@@ -180,6 +184,11 @@ class Vanka:
 
     def vmult(self, dst, src, stream=None):
         check(lib().stmg_vanka_vmult(self.h, _dev(dst), _dev(src), _stream(stream)))
+
+    def step(self, op, omega, x, b, tmp, stream=None):
+        """x += omega P (b - A x) (stmg_relax_step); tmp receives b - A x."""
+        check(lib().stmg_relax_step(self.h, op.h, C.c_double(omega), _dev(x), _dev(b), _dev(tmp),
+                                    _stream(stream)))
 
 
 class Transfer:
@@ -280,6 +289,23 @@ class Solver:
     def set_source(self, f_nodal):
         f = np.ascontiguousarray(f_nodal, dtype=np.float64)
         check(lib().stmg_solver_set_source(self.h, _ptr(f)))
+
+    def point_values(self, points, samples_per_step=0, stream=None):
+        """u of the last slab at the points for samples_per_step equidistant
+        times per step (stmg_solver_point_values); returns (times, values)
+        with values of shape (n_steps * samples, n_points)."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, self.cfg.dim)
+        r = self.cfg.time_degree
+        samples = samples_per_step if samples_per_step > 0 else (r + 1) ** 2
+        rows = self.cfg.n_steps * samples
+        times, vals = np.zeros(rows), np.zeros((rows, pts.shape[0]))
+        check(lib().stmg_solver_point_values(self.h, pts.shape[0], _ptr(pts), samples, _ptr(times), _ptr(vals),
+                                             _stream(stream)))
+        return times, vals
+
+    def set_control(self, tol, abs_tol, max_iter):
+        """FGMRES ReductionControl of the following slabs (stmg_solver_set_control)."""
+        check(lib().stmg_solver_set_control(self.h, C.c_double(tol), C.c_double(abs_tol), int(max_iter)))
 
     def run(self, n_slabs, stream=None):
         its = np.zeros(n_slabs, dtype=np.int32)

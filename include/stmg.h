@@ -77,6 +77,17 @@ STMG_API int stmg_time_weights(int time_type, int r, double tau, int n_steps, in
  * restriction is the transpose (gmg.h:77-136 with restrict_is_transpose). */
 STMG_API int stmg_time_transfer(int time_type, int kind, int r, int n_steps, double *P);
 
+/* Reorders block vectors between a caller's dof numbering and the library's
+ * lexicographic node order, per time block: dst[b][i] = src[b][perm[i]]
+ * (scatter = 0, caller order -> lexicographic when perm[i] is the caller's
+ * index of lexicographic node i) or dst[b][perm[i]] = src[b][i] (scatter =
+ * 1, back). perm: device array of n indices; src, dst: device, n_blocks x n,
+ * distinct. The adapter a deal.II caller needs around every call (its
+ * DoFHandler numbers the dofs of a BlockVector block, tests/tp_01.cc:260-285);
+ * no counterpart in the reference. */
+STMG_API int stmg_block_permute(int n_blocks, long long n, const long long *perm, int scatter, const void *src,
+                                void *dst, int dtype, void *stream);
+
 /* ---------------------------------------------------------------- mesh
  * Structured hex mesh of n_cells[0] x n_cells[1] (x n_cells[2]) cells of
  * FE_Q(degree) on Gauss-Lobatto nodes with MappingQ1 and homogeneous
@@ -124,6 +135,14 @@ STMG_API int stmg_op_vmult(stmg_op_t op, void *dst, const void *src, void *strea
 STMG_API int stmg_op_vmult_box_noalloc(int dim, const int *n_cells, int degree, const double *lo, const double *hi,
                                        const void *coeff, int nt_out, int nt_in, const double *A, const double *B,
                                        int dtype, void *dst, const void *src, void *stream);
+/* SystemMatrix::get_matrix_diagonal (inverse = 0) or
+ * get_matrix_diagonal_inverse (inverse = 1), operators.h:188-215: block i
+ * of dst (n_t x n_nodes, the operator's dtype) is A(i,i) diag(K) +
+ * B(i,i) diag(M), or diag(K)^+ / A(i,i) + diag(M)^+ / B(i,i) with x^+ = 1/x
+ * where |x| > sqrt(eps) and 1 elsewhere (MatrixFreeOperator::
+ * compute_diagonal, operators.h:467-485). Dirichlet rows of diag(K) and
+ * diag(M) are 1. Square operators only. */
+STMG_API int stmg_op_diagonal(stmg_op_t op, int inverse, void *dst, void *stream);
 /* SystemMatrix::Tvmult (operators.h:124-152): A and B transposed. */
 STMG_API int stmg_op_Tvmult(stmg_op_t op, void *dst, const void *src, void *stream);
 /* SystemMatrix::vmult_add (operators.h:155-180): dst += op(src). */
@@ -142,6 +161,13 @@ STMG_API int stmg_vanka_create(stmg_mesh_t mesh, int nt, const double *Alpha, co
 STMG_API int stmg_vanka_destroy(stmg_vanka_t vanka);
 /* PreconditionVanka::vmult (gmg.h:476-514): dst = sum_c R_c^T D_c B_c^{-1} R_c src. */
 STMG_API int stmg_vanka_vmult(stmg_vanka_t vanka, void *dst, const void *src, void *stream);
+
+/* PreconditionRelaxation<SystemMatrix, PreconditionVanka>::step, the
+ * smoother sweep of MGSmootherPrecondition (gmg.h:660-664,714-730):
+ * x += omega P_vanka (b - A x); tmp (same shape) receives b - A x. The
+ * operator and the smoother must be of one mesh, n_t and compute type. */
+STMG_API int stmg_relax_step(stmg_vanka_t vanka, stmg_op_t op, double omega, void *x, const void *b, void *tmp,
+                             void *stream);
 
 /* ------------------------------------------------------------ transfers
  * h: between a mesh and its 2x refinement (same degree), nt time blocks;
@@ -191,6 +217,21 @@ STMG_API int stmg_solver_set_initial(stmg_solver_t solver, const double *u0, con
 /* replace the nodal source field (host array of n_nodes; rhs_mode 1): the
  * integrate_rhs_function of tests/tp_01.cc:390-398 for an FE source */
 STMG_API int stmg_solver_set_source(stmg_solver_t solver, const double *f_nodal);
+/* Point functionals of the last slab run (tests/tp_01.cc:451-619): the
+ * displacement / temperature u at n_points points (host, n_points x dim,
+ * inside the mesh) for every time node of each step (RemotePointEvaluation
+ * with FEPointEvaluation under the Q1 map), mapped by the time evaluation
+ * matrix (get_time_evaluation_matrix, fe_time.h:250-267) to samples_per_step
+ * equidistant times per step (<= 0: (r+1)^2 as the reference); cGP steps
+ * take the step's initial value as their first node. values (host):
+ * (n_steps samples) x n_points, row-major; times (host, may be NULL):
+ * n_steps samples. */
+STMG_API int stmg_solver_point_values(stmg_solver_t solver, int n_points, const double *points, int samples_per_step,
+                                      double *times, double *values, void *stream);
+/* the FGMRES ReductionControl of the following slabs (time_integrators.h:44:
+ * max_iter, abs_tol, tol as a reduction of the initial residual), as a
+ * caller changes a deal.II SolverControl between solves */
+STMG_API int stmg_solver_set_control(stmg_solver_t solver, double tol, double abs_tol, int max_iter);
 /* the slab loop of tests/tp_01.cc:630-683 with TimeIntegratorHeat::solve /
  * TimeIntegratorWave::solve (time_integrators.h:157-180,237-280);
  * iterations: host array of n_slabs FGMRES counts (may be NULL) */

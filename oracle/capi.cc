@@ -248,8 +248,17 @@ extern "C"
     });
   }
 
+  int orc_run_all(const OrcConfig *c, OrcResult *res, int *iterations, double *u_last, double *v_last, double *u_all);
+
   int
   orc_run(const OrcConfig *c, OrcResult *res, int *iterations, double *u_last, double *v_last)
+  {
+    return orc_run_all(c, res, iterations, u_last, v_last, nullptr);
+  }
+
+  // orc_run, and with u_all non-null every slab's blocks (n_slabs x n_blocks x N)
+  int
+  orc_run_all(const OrcConfig *c, OrcResult *res, int *iterations, double *u_last, double *v_last, double *u_all)
   {
     return guard([&] {
       Config cfg;
@@ -283,6 +292,7 @@ extern "C"
       cfg.tol                   = c->tol;
       cfg.abs_tol               = c->abs_tol;
       cfg.frequency             = c->frequency;
+      cfg.keep_all              = u_all != nullptr;
       const int nf[3]           = {c->subdiv[0] << c->refine, c->subdiv[1] << c->refine, c->subdiv[2] << c->refine};
       std::size_t nn = 1, nc = 1, nv = 1;
       for (int d = 0; d < c->dim; ++d)
@@ -316,6 +326,8 @@ extern "C"
         std::copy(r.u_last.begin(), r.u_last.end(), u_last);
       if (v_last)
         std::copy(r.v_last.begin(), r.v_last.end(), v_last);
+      if (u_all)
+        std::copy(r.u_all.begin(), r.u_all.end(), u_all);
     });
   }
 }

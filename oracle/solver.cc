@@ -840,6 +840,8 @@ namespace oracle
                   res.l8 = std::max(res.l8, l8);
                 }
           }
+        if (cfg.keep_all)
+          res.u_all.insert(res.u_all.end(), x.begin(), x.end());
         time += cfg.n_steps * tau;
       }
     res.l2     = std::sqrt(res.l2);

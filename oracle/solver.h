@@ -60,6 +60,7 @@ namespace oracle
     std::vector<double> fine_coeff;    // empty = 1; else per finest cell
     bool                compute_errors = true;
     bool                mg_float       = true; // FP32 V-cycle (tests/tp_01.cc:767,776)
+    bool                keep_all       = false; // Result::u_all: every slab's blocks
   };
 
   struct Result
@@ -69,6 +70,7 @@ namespace oracle
     double              l8 = -1, l2 = 0, h1 = 0; // L-inf-L-inf, L2-L2, L2-H1semi
     std::vector<double> omega;                   // per level
     std::vector<double> u_last;                  // all blocks of the last slab
+    std::vector<double> u_all;                   // all blocks of every slab (Config::keep_all)
     std::vector<double> v_last;
     std::size_t         n_dofs = 0, n_cells = 0;
     int                 n_blocks = 0, n_levels = 0;

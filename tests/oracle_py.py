@@ -67,6 +67,7 @@ def lib():
         L.orc_time_weights.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
         L.orc_time_prolongation.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _dp]
         L.orc_run.argtypes = [C.POINTER(OrcConfig), C.POINTER(OrcResult), _ip, _dp, _dp]
+        L.orc_run_all.argtypes = [C.POINTER(OrcConfig), C.POINTER(OrcResult), _ip, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -192,7 +193,9 @@ def time_prolongation(ttype, kind, r, n_steps):
 def run(dim=2, subdiv=(1, 1, 1), refine=2, p=2, r=1, ttype=DG, problem=HEAT, n_steps=1, n_slabs=None, tau=None,
         fe_degree_min=-1, n_steps_min=-1, mg_float=True, tol=1e-12, abs_tol=1e-12, frequency=1.0, rhs_mode=0,
         f_nodal=None, u0_nodal=None, v0_nodal=None, fine_vertices=None, fine_coeff=None, compute_errors=True,
-        smoothing_steps=1, extrapolate=True, max_iter=200, lo=(0, 0, 0), hi=(1, 1, 1)):
+        smoothing_steps=1, extrapolate=True, max_iter=200, lo=(0, 0, 0), hi=(1, 1, 1), keep_all=False):
+    """The oracle's slab loop; with keep_all the result's "u_all" holds every
+    slab's blocks (n_slabs, n_blocks * n_nodes)."""
     if tau is None:
         tau = 2.0 ** -(refine + 1)
     if n_slabs is None:
@@ -225,6 +228,7 @@ def run(dim=2, subdiv=(1, 1, 1), refine=2, p=2, r=1, ttype=DG, problem=HEAT, n_s
     nb = (r + 1 if ttype == DG else r) * n_steps
     u = np.zeros(nb * nn)
     v = np.zeros(nb * nn)
-    _check(lib().orc_run(C.byref(c), C.byref(res), its.ctypes.data_as(_ip), _ptr(u), _ptr(v)))
+    u_all = np.zeros((n_slabs, nb * nn)) if keep_all else None
+    _check(lib().orc_run_all(C.byref(c), C.byref(res), its.ctypes.data_as(_ip), _ptr(u), _ptr(v), _ptr(u_all)))
     return dict(iterations=its, total_iterations=res.total_iterations, n_levels=res.n_levels, linf=res.l8,
-                l2=res.l2, h1=res.h1, n_dofs=res.n_dofs, n_cells=res.n_cells, u=u, v=v)
+                l2=res.l2, h1=res.h1, n_dofs=res.n_dofs, n_cells=res.n_cells, u=u, v=v, u_all=u_all)

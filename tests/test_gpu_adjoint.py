@@ -124,3 +124,54 @@ def test_gradient_3d_matches_finite_differences():
     h = 1e-4
     fd = (misfit(theta + h * d) - misfit(theta - h * d)) / (2 * h)
     assert abs(g @ d - fd) <= 1e-6 * max(abs(fd), abs(g @ d)), (g @ d, fd)
+
+
+def test_autograd_wrapper_gradcheck_small():
+    """The torch.autograd.Function wrapper (stmg.adjoint.misfit) passes
+    torch.autograd.gradcheck (central differences in every parameter) on a
+    small problem: 2-D 4x4 Q2 cells, dG(1), three slabs."""
+    import stmg
+    from stmg.adjoint import misfit
+    rng = np.random.default_rng(81)
+    n = 4
+    nn = (2 * n + 1) ** 2
+    f = rng.standard_normal(nn)
+    f[meshes.boundary_mask(2, (n, n), 2)] = 0.0
+    obs = 0.1 * rng.standard_normal((SLABS, 2 * nn))
+    obs[:, np.tile(meshes.boundary_mask(2, (n, n), 2), 2)] = 0.0
+    kw = dict(BASE, refine=2)
+
+    def make(kappa):
+        return stmg.Solver(time_type=stmg.DG, problem=stmg.HEAT, mg_dtype=stmg.F64, f_nodal=f, fine_coeff=kappa, **kw)
+
+    theta = torch.tensor(rng.normal(0.0, 0.5, n * n), dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(lambda th: misfit(th, make, obs), (theta,), eps=1e-5, atol=1e-9, rtol=1e-5)
+
+
+def test_autograd_wrapper_directional_fd_3d():
+    """J.backward() through the wrapper against central differences of
+    forward solves on random unit directions (3-D 4^3 Q2 cells, dG(1), four
+    slabs, checkpoints every two slabs)."""
+    import stmg
+    from stmg.adjoint import misfit, misfit_value
+    rng = np.random.default_rng(82)
+    n, S = 4, 4
+    nn = (2 * n + 1) ** 3
+    f = np.ones(nn)
+    obs = 0.05 * rng.standard_normal((S, 2 * nn))
+    obs[:, np.tile(meshes.boundary_mask(3, (n, n, n), 2), 2)] = 0.0
+    kw = dict(BASE, dim=3, refine=2, tau=1 / 16)
+
+    def make(kappa):
+        return stmg.Solver(time_type=stmg.DG, problem=stmg.HEAT, mg_dtype=stmg.F64, f_nodal=f, fine_coeff=kappa, **kw)
+
+    theta = torch.zeros(n ** 3, dtype=torch.float64, requires_grad=True)
+    J = misfit(theta, make, obs, 2)
+    J.backward()
+    g = theta.grad.numpy()
+    h = 1e-4
+    for _ in range(3):
+        d = rng.standard_normal(n ** 3)
+        d /= np.linalg.norm(d)
+        fd = (misfit_value(h * d, make, obs) - misfit_value(-h * d, make, obs)) / (2 * h)
+        assert abs(g @ d - fd) <= 1e-6 * abs(fd), (g @ d, fd)

@@ -97,3 +97,76 @@ def test_operator_deterministic():
     op.vmult(d1, s)
     op.vmult(d2, s)
     assert torch.equal(d1, d2)
+
+
+def _assembled_diagonals(om, dim, n, p):
+    """Diagonals of K and M summed over the oracle's element matrices
+    (interior nodes; Dirichlet rows are left to the caller)."""
+    from test_oracle_operator import cell_dofs
+    nn = list(n) + [1] * (3 - len(n))
+    dK, dM = np.zeros(om.n_nodes), np.zeros(om.n_nodes)
+    for c in range(int(np.prod(n))):
+        K, M = om.element_matrices(c)
+        g = cell_dofs(dim, nn, p, c)
+        np.add.at(dK, g, np.diag(K))
+        np.add.at(dM, g, np.diag(M))
+    return dK, dM
+
+
+@pytest.mark.parametrize("case", [CASES[i] for i in (1, 2, 3, 7, 8, 9, 14)],
+                         ids=lambda c: f"d{c[0]}-{'x'.join(map(str, c[1]))}-p{c[2]}-dist{c[3]}-c{c[4]}")
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_operator_diagonal_matches_assembled(case, prec):
+    """stmg_op_diagonal (get_matrix_diagonal[_inverse], operators.h:188-215)
+    against the diagonals of the assembled element matrices; Dirichlet rows
+    of diag(K) and diag(M) are 1; the inverse follows the reference's
+    composition diag(K)^+ / Alpha(i,i) + diag(M)^+ / Beta(i,i)."""
+    import stmg
+    om, gm, A, B, _, _ = build(case)
+    dim, n, p = case[0], case[1], case[2]
+    nt = A.shape[0]
+    dK, dM = _assembled_diagonals(om, dim, n, p)
+    bd = meshes.boundary_mask(dim, n, p)
+    dK[bd], dM[bd] = 1.0, 1.0
+    ref = np.concatenate([A[j, j] * dK + B[j, j] * dM for j in range(nt)])
+    eps = np.finfo(np.float64 if prec == "f64" else np.float32).eps
+    inv = lambda d: np.where(np.abs(d) > np.sqrt(eps), 1.0 / d, 1.0)
+    ref_inv = np.concatenate([inv(dK) / A[j, j] + inv(dM) / B[j, j] for j in range(nt)])
+    op = stmg.Operator(gm, A, B, dtype=stmg.F64 if prec == "f64" else stmg.F32)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    d = torch.zeros(nt * om.n_nodes, dtype=dt, device="cuda")
+    tol = 1e-12 if prec == "f64" else 2e-6
+    op.diagonal(d)
+    assert rel_err(d.double().cpu().numpy(), ref) < tol
+    op.diagonal(d, inverse=True)
+    assert rel_err(d.double().cpu().numpy(), ref_inv) < tol
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_relax_step_matches_composition(prec):
+    """stmg_relax_step: x + omega P (b - A x), against the operator and the
+    smoother applied one after the other."""
+    import stmg
+    om, gm, A, B, _, _ = build(CASES[7])
+    dim, n, p = 3, CASES[7][1], 2
+    nt = A.shape[0]
+    mask = meshes.boundary_mask(dim, n, p)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    mode = stmg.F64 if prec == "f64" else stmg.F32
+    op = stmg.Operator(gm, A, B, dtype=mode)
+    vk = stmg.Vanka(gm, A, B, compute=mode, storage=mode)
+    x = torch.tensor(meshes.random_block_vector(nt, om.n_nodes, mask, seed=61), dtype=dt, device="cuda")
+    b = torch.tensor(meshes.random_block_vector(nt, om.n_nodes, mask, seed=62), dtype=dt, device="cuda")
+    omega = 0.7
+    r, pr = torch.empty_like(x), torch.empty_like(x)
+    op.vmult(r, x)
+    r = b - r
+    vk.vmult(pr, r)
+    ref = x + omega * pr
+    tmp = torch.empty_like(x)
+    x1 = x.clone()
+    vk.step(op, omega, x1, b, tmp)
+    torch.cuda.synchronize()
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert torch.linalg.norm(x1 - ref) <= tol * torch.linalg.norm(ref)
+    assert torch.linalg.norm(tmp - r) <= tol * torch.linalg.norm(r)
