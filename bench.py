@@ -249,11 +249,18 @@ def accuracy_report(u32, u64, uref, tol):
     return rep
 
 
-def kernel_roofline(stmg, torch, w, kappa, hbm, only=None, fp64=False):
+def vanka_record_bytes(storage_bf16):
+    """Bytes of one Q2 cell's Vanka record read per apply: V (27 x 27) in the
+    storage type and the 27 FP32 eigenvalues (padding excluded)."""
+    return 27 * 27 * (2 if storage_bf16 else 4) + 27 * 4
+
+
+def kernel_roofline(stmg, torch, w, kappa, hbm, only=None, fp64=False, bf16=False):
     """Finest-level FP32 operator and Vanka apply timed in isolation with CUDA
     events on the launching stream; algorithmic bytes per launch:
       operator: 2 n_t N 4 (read src, write dst) + cells 4 (coefficient)
-      Vanka:    cells (nd^2 + nd) 4 (eigenvectors, eigenvalues) + 2 n_t N 4."""
+      Vanka:    cells (nd^2 s + nd 4) (eigenvectors in the storage type s,
+                eigenvalues) + 2 n_t N 4."""
     n = 1 << w["refine"]
     mesh = stmg.Mesh(3, (n, n, n), 2, coeff=kappa)
     A, B, _, _, _ = stmg.time_weights(stmg.DG, 3, w["tau"], 1, stmg.HEAT)
@@ -263,10 +270,11 @@ def kernel_roofline(stmg, torch, w, kappa, hbm, only=None, fp64=False):
     s = torch.cuda.current_stream()
     out = {}
     op = stmg.Operator(mesh, A, B, dtype=stmg.F64 if fp64 else stmg.F32) if only in (None, "st_apply") else None
-    vk = stmg.Vanka(mesh, A, B, compute=stmg.F32, storage=stmg.F32) if only in (None, "vanka_apply") else None
+    vk = stmg.Vanka(mesh, A, B, compute=stmg.F32, storage=stmg.BF16 if bf16 else stmg.F32) \
+        if only in (None, "vanka_apply") else None
     sz = 8 if fp64 else 4
     for name, fn, nbytes in (("st_apply", lambda: op.vmult(y, x), 2 * nt * N * sz + w["cells"] * sz),
-                             ("vanka_apply", lambda: vk.vmult(y, x), w["cells"] * (27 * 27 + 27) * 4 + 2 * nt * N * 4)):
+                             ("vanka_apply", lambda: vk.vmult(y, x), w["cells"] * vanka_record_bytes(bf16) + 2 * nt * N * 4)):
         if only is not None and name != only:
             continue
         for _ in range(3):
@@ -304,10 +312,14 @@ def run_ours(args):
     kappa, f = inputs(w, SEED + rank)
     hbm, hbm_kind = peaks()
 
+    bf16 = args.vanka_storage == "bf16"
+
     def make(mg_dtype, tol=w["tol"], max_iter=200):
+        storage = None if mg_dtype == stmg.F64 else (stmg.BF16 if bf16 else stmg.F32)
         return stmg.Solver(dim=3, refine=w["refine"], degree=2, time_degree=3, time_type=stmg.DG,
                            problem=stmg.HEAT, n_steps=1, tau=w["tau"], mg_dtype=mg_dtype, tol=tol,
-                           abs_tol=1e-300, rhs_mode=1, f_nodal=f, fine_coeff=kappa, max_iter=max_iter)
+                           abs_tol=1e-300, rhs_mode=1, f_nodal=f, fine_coeff=kappa, max_iter=max_iter,
+                           vanka_storage=storage)
 
     n_acc = 0 if args.no_accuracy else w["n_slabs"]
 
@@ -387,7 +399,7 @@ def run_ours(args):
         accuracy = accuracy_report(u32, u64, uref, w["tol"])
     del u32, u64
 
-    kr = kernel_roofline(stmg, torch, w, kappa, hbm)
+    kr = kernel_roofline(stmg, torch, w, kappa, hbm, bf16=bf16)
     dom = max(kr, key=lambda k: kr[k]["ms"])
     traffic = vanka_traffic(w["refine"]) if dom == "vanka_apply" else None
     roof = dict(kernel=dom, bound="hbm", achieved=kr[dom]["achieved"], peak=hbm, unit="GB/s",
@@ -405,6 +417,7 @@ def run_ours(args):
                     dtype="f32", data="synthetic",
                     config=dict(workload=w["name"], cells=w["cells"], nodes=w["nodes"], time_dofs=w["nt"],
                                 dofs_per_slab=dofs_step, outer="fgmres-fp64", mg="fp32 v-cycle, cell-patch vanka",
+                                vanka_storage=args.vanka_storage,
                                 tol=w["tol"], l2="inputs larger than L2 (FGMRES basis 30 x 0.54 GB)",
                                 parallelism="replicas" if world > 1 else "single-gpu", setup_s=t_setup),
                     fgmres_iterations=[int(i) for i in its32], e2e=e2e, roofline=roof, cpu_baseline=cpu,
@@ -608,6 +621,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--refine", type=int, default=7, help="mesh 2^refine cells per direction (7: 128^3)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 V-cycle comparison")
+    ap.add_argument("--vanka-storage", choices=["f32", "bf16"], default="f32",
+                    help="storage of the FP32 V-cycle's Vanka eigenvectors")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the per-slab comparison of the FP32-MG and FP64-MG solutions with a converged "
@@ -633,7 +648,8 @@ def main():
         kappa, _ = inputs(w)
         hbm, kind = peaks()
         only = None if args.kernels_only == "all" else args.kernels_only.replace("64", "")
-        kr = kernel_roofline(stmg, torch, w, kappa, hbm, only, fp64=args.kernels_only == "st_apply64")
+        kr = kernel_roofline(stmg, torch, w, kappa, hbm, only, fp64=args.kernels_only == "st_apply64",
+                             bf16=args.vanka_storage == "bf16")
         print(json.dumps(dict(workload=w["name"], peak_gbs=hbm, peak_kind=kind, kernels=kr)), flush=True)
         return 0
     if args.impl == "reference":

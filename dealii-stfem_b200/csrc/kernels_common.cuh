@@ -2,6 +2,8 @@
 // tensor-product sweeps, Q1 geometry, node indexing and the tile shell.
 #pragma once
 
+#include <algorithm>
+
 #include "stmg_internal.h"
 
 namespace stmg
@@ -258,94 +260,102 @@ namespace stmg
   // Fix-up of the nodes the tiles share, visited by family: nodes on
   // interior x tile planes (owned by the tiles' x faces), then y planes
   // (minus x-plane nodes), then z planes (minus x- and y-plane nodes), then
-  // the Dirichlet faces (each node once). Consecutive items walk a plane row,
-  // so the face-slot reads are coalesced.
+  // the Dirichlet faces (each node once). One block takes a segment of one
+  // row of one plane: the plane (and its family) comes from blockIdx.z, the
+  // row from blockIdx.y, the position along the row from the thread, so no
+  // node index is decoded by division; along y and z planes the rows run
+  // along x (coalesced writes of dst).
   struct FixupRanges
   {
-    long long nx, ny, nz, nb;
-    long long total() const { return nx + ny + nz + nb; }
+    int nxp, nyp, nzp, nfaces; // interior planes per direction, Dirichlet faces
+    int rows, seg;             // grid extents: rows, row segments of FIXUP_THREADS
+    int planes() const { return nxp + nyp + nzp + nfaces; }
   };
+
+  constexpr int FIXUP_THREADS = 128;
 
   inline FixupRanges
   fixup_ranges(const MeshView &m, const Tiling &tl)
   {
-    const long long n0 = m.nn[0], n1 = m.nn[1], n2 = m.nn[2];
-    FixupRanges     r;
-    r.nx = (long long)(tl.ntiles[0] - 1) * n1 * n2;
-    r.ny = (long long)(tl.ntiles[1] - 1) * n0 * n2;
-    r.nz = m.dim == 3 ? (long long)(tl.ntiles[2] - 1) * n0 * n1 : 0;
-    r.nb = 2 * n1 * n2 + 2 * (n0 - 2) * n2 + (m.dim == 3 ? 2 * (n0 - 2) * (n1 - 2) : 0);
+    FixupRanges r;
+    r.nxp    = tl.ntiles[0] - 1;
+    r.nyp    = tl.ntiles[1] - 1;
+    r.nzp    = m.dim == 3 ? tl.ntiles[2] - 1 : 0;
+    r.nfaces = m.dim == 3 ? 6 : 4;
+    r.rows   = std::max(m.nn[1], m.nn[2]);
+    r.seg    = (std::max(m.nn[0], m.nn[1]) + FIXUP_THREADS - 1) / FIXUP_THREADS;
     return r;
   }
 
+  // floor(g / span) for 0 <= g < 2^24 and the span's reciprocal rs
+  __device__ __forceinline__ int
+  div_span(int g, int span, float rs)
+  {
+    int q = __float2int_rd(float(g) * rs);
+    if (q * span > g)
+      --q;
+    else if ((q + 1) * span <= g)
+      ++q;
+    return q;
+  }
+
   template <int DIM, typename T, bool WEIGHTED>
-  __global__ void
+  __global__ void __launch_bounds__(FIXUP_THREADS)
   plane_fixup_kernel(const MeshView m, const Tiling tl, int nt, const T *__restrict__ shell, T *__restrict__ dst,
                      const OutMode<T> om, const FixupRanges rg)
   {
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int n0 = m.nn[0], n1 = m.nn[1], n2 = m.nn[2];
-    const int sx = tl.T[0] * m.p, sy = tl.T[1] * m.p, sz = tl.T[2] * m.p;
+    const int span[3] = {tl.T[0] * m.p, tl.T[1] * m.p, tl.T[2] * m.p};
+    int       pl = blockIdx.z, row = blockIdx.y, pos = blockIdx.x * FIXUP_THREADS + threadIdx.x;
     int       g[3];
     bool      boundary = false;
-    if (i < rg.nx)
+    if (pl < rg.nxp)
       {
-        const long long pl = (long long)n1 * n2;
-        g[0]               = int(1 + i / pl) * sx;
-        const long long r  = i % pl;
-        g[1]               = int(r % n1);
-        g[2]               = int(r / n1);
+        // x plane: rows z, positions y
+        if (row >= n2 || pos >= n1)
+          return;
+        g[0] = (pl + 1) * span[0], g[1] = pos, g[2] = row;
       }
-    else if ((i -= rg.nx) < rg.ny)
+    else if ((pl -= rg.nxp) < rg.nyp)
       {
-        const long long pl = (long long)n0 * n2;
-        g[1]               = int(1 + i / pl) * sy;
-        const long long r  = i % pl;
-        g[0]               = int(r % n0);
-        g[2]               = int(r / n0);
-        if (g[0] % sx == 0)
-          return; // on an x plane
+        // y plane: rows z, positions x
+        if (row >= n2 || pos >= n0 || pos % span[0] == 0)
+          return; // on an x plane or the x faces
+        g[0] = pos, g[1] = (pl + 1) * span[1], g[2] = row;
       }
-    else if ((i -= rg.ny) < rg.nz)
+    else if ((pl -= rg.nyp) < rg.nzp)
       {
-        const long long pl = (long long)n0 * n1;
-        g[2]               = int(1 + i / pl) * sz;
-        const long long r  = i % pl;
-        g[0]               = int(r % n0);
-        g[1]               = int(r / n0);
-        if (g[0] % sx == 0 || g[1] % sy == 0)
-          return; // on an x or y plane
+        // z plane: rows y, positions x
+        if (row >= n1 || pos >= n0 || pos % span[0] == 0 || row % span[1] == 0)
+          return;
+        g[0] = pos, g[1] = row, g[2] = (pl + 1) * span[2];
       }
-    else if ((i -= rg.nz) < rg.nb)
+    else
       {
+        // Dirichlet faces, each node once: x faces whole, y faces without
+        // the x faces' nodes, z faces without both
+        pl -= rg.nzp;
         boundary = true;
-        // x faces (all nodes), y faces (x interior), z faces (x, y interior)
-        const long long fx = 2ll * n1 * n2, fy = 2ll * (n0 - 2) * n2;
-        if (i < fx)
+        const int f = pl >> 1, hi = pl & 1;
+        if (f == 0)
           {
-            g[0] = (i < (long long)n1 * n2) ? 0 : n0 - 1;
-            const long long r = i % ((long long)n1 * n2);
-            g[1]              = int(r % n1);
-            g[2]              = int(r / n1);
+            if (row >= n2 || pos >= n1)
+              return;
+            g[0] = hi ? n0 - 1 : 0, g[1] = pos, g[2] = row;
           }
-        else if ((i -= fx) < fy)
+        else if (f == 1)
           {
-            g[1] = (i < (long long)(n0 - 2) * n2) ? 0 : n1 - 1;
-            const long long r = i % ((long long)(n0 - 2) * n2);
-            g[0]              = 1 + int(r % (n0 - 2));
-            g[2]              = int(r / (n0 - 2));
+            if (row >= n2 || pos < 1 || pos >= n0 - 1)
+              return;
+            g[0] = pos, g[1] = hi ? n1 - 1 : 0, g[2] = row;
           }
         else
           {
-            i -= fy;
-            g[2] = (i < (long long)(n0 - 2) * (n1 - 2)) ? 0 : n2 - 1;
-            const long long r = i % ((long long)(n0 - 2) * (n1 - 2));
-            g[0]              = 1 + int(r % (n0 - 2));
-            g[1]              = 1 + int(r / (n0 - 2));
+            if (row < 1 || row >= n1 - 1 || pos < 1 || pos >= n0 - 1)
+              return;
+            g[0] = pos, g[1] = row, g[2] = hi ? n2 - 1 : 0;
           }
       }
-    else
-      return;
     const long long node = g[0] + (long long)n0 * (g[1] + (long long)n1 * g[2]);
     if (boundary)
       {
@@ -375,12 +385,12 @@ namespace stmg
             tt0[d] = 0, ll0[d] = 0, two[d] = 0, ee0[d] = ee1[d] = 1;
             continue;
           }
-        const int span = tl.T[d] * m.p;
-        two[d]         = g[d] % span == 0; // interior node on a tile plane (boundary nodes returned above)
-        tt0[d]         = two[d] ? g[d] / span - 1 : min(g[d] / span, tl.ntiles[d] - 1);
-        ll0[d]         = g[d] - tt0[d] * span;
-        ee0[d]         = min(tl.T[d], m.n[d] - tt0[d] * tl.T[d]) * m.p + 1;
-        ee1[d]         = two[d] ? min(tl.T[d], m.n[d] - (tt0[d] + 1) * tl.T[d]) * m.p + 1 : 1;
+        const int q = div_span(g[d], span[d], 1.0f / float(span[d]));
+        two[d]      = q * span[d] == g[d]; // interior node on a tile plane (boundary nodes returned above)
+        tt0[d]      = two[d] ? q - 1 : min(q, tl.ntiles[d] - 1);
+        ll0[d]      = g[d] - tt0[d] * span[d];
+        ee0[d]      = min(tl.T[d], m.n[d] - tt0[d] * tl.T[d]) * m.p + 1;
+        ee1[d]      = two[d] ? min(tl.T[d], m.n[d] - (tt0[d] + 1) * tl.T[d]) * m.p + 1 : 1;
       }
     long long off[8];
     bool      ok[8];
@@ -395,15 +405,22 @@ namespace stmg
                            shell_slot<DIM>(tl, e, ix ? 0 : ll0[0], iy ? 0 : ll0[1], iz ? 0 : ll0[2])
                        : 0;
       }
-    long long gi = node;
-    for (int j = 0; j < nt; ++j, gi += m.N)
+    // four time dofs at a time with all their face-slot loads in flight
+    // (each node's sum still runs over the tiles in the fixed order c)
+    for (int j0 = 0; j0 < nt; j0 += 4)
       {
-        T s = T(0);
+        T s[4] = {T(0), T(0), T(0), T(0)};
 #pragma unroll
         for (int c = 0; c < 8; ++c)
           if (ok[c])
-            s += shell[off[c] + (long long)j * tl.tile_stride];
-        om.write(dst, gi, s * w);
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj)
+              if (j0 + jj < nt)
+                s[jj] += shell[off[c] + (long long)(j0 + jj) * tl.tile_stride];
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj)
+          if (j0 + jj < nt)
+            om.write(dst, node + (long long)(j0 + jj) * m.N, s[jj] * w);
       }
   }
 
@@ -413,10 +430,10 @@ namespace stmg
                      cudaStream_t s)
   {
     const FixupRanges rg = fixup_ranges(m, tl);
-    const long long   n  = rg.total();
-    if (n <= 0)
+    if (rg.planes() <= 0)
       return;
-    plane_fixup_kernel<DIM, T, WEIGHTED><<<unsigned((n + 255) / 256), 256, 0, s>>>(m, tl, nt, shell, dst, om, rg);
+    const dim3 grid(unsigned(rg.seg), unsigned(rg.rows), unsigned(rg.planes()));
+    plane_fixup_kernel<DIM, T, WEIGHTED><<<grid, FIXUP_THREADS, 0, s>>>(m, tl, nt, shell, dst, om, rg);
     count_launch();
     STMG_CUDA(cudaGetLastError());
   }

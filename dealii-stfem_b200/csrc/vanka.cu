@@ -90,7 +90,8 @@ namespace stmg
     vanka_setup_kernel(const MeshView m, const double *__restrict__ Kref, const double *__restrict__ Mref,
                        const double *__restrict__ elemK, const double *__restrict__ elemM,
                        unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int mu_double,
-                       int *__restrict__ status, const Tiling tl, int tiled, int row_stride, int mu_stride)
+                       int *__restrict__ status, const Tiling tl, int tiled, int row_stride, int mu_stride,
+                       int swz_kt)
     {
       constexpr int P1 = P + 1;
       constexpr int ND = Tens<P1, DIM>::ND;
@@ -325,7 +326,12 @@ namespace stmg
       for (int e = tid; e < ND * ND; e += nth)
         {
           const int mm = e / ND, a = e % ND;
-          reinterpret_cast<TS *>(rec + slot * rec_bytes)[mm * row_stride + a] = to_storage<TS>(Q[a][mm]);
+          if (swz_kt == 32)
+            *reinterpret_cast<TS *>(rec + slot * rec_bytes + MmaRows<32>::offset(mm, a)) = to_storage<TS>(Q[a][mm]);
+          else if (swz_kt == 16)
+            *reinterpret_cast<TS *>(rec + slot * rec_bytes + MmaRows<16>::offset(mm, a)) = to_storage<TS>(Q[a][mm]);
+          else
+            reinterpret_cast<TS *>(rec + slot * rec_bytes)[mm * row_stride + a] = to_storage<TS>(Q[a][mm]);
         }
     }
 
@@ -418,8 +424,11 @@ namespace stmg
     if (streamed)
       {
         const std::size_t ntp = nt == 3 ? 4 : nt;
+        if (mmarec)
+          return std::size_t(stages) * colour_cells * rec_bytes + 4 * 3 * nb * ntp +
+                 vanka_detail::VR_WARPS * 32 * 16 + 128;
         if (rowrec)
-          return std::size_t(vanka_detail::VR_STAGES) * colour_cells * rec_bytes +
+          return std::size_t(stages) * colour_cells * rec_bytes +
                  4 * (3 * nb * ntp + vanka_detail::VR_WARPS * std::size_t(mesh->nd) * ntp);
         return std::size_t(vanka_detail::VK_STAGES) * colour_cells * rec_bytes +
                4 * (3 * nb * ntp + 8 * std::size_t(mesh->nd) * ntp);
@@ -482,7 +491,8 @@ namespace stmg
         (void)Vp;
         kern<<<unsigned(m.ncells), threads, smem>>>(m, Kref.ptr, Mref.ptr, eK.ptr, eM.ptr, vk.V.ptr, vk.rec_bytes,
                                                     vk.mu_off, vk.compute == STMG_F64 ? 1 : 0, status.ptr, vk.tiling,
-                                                    vk.streamed ? 1 : 0, vk.row_stride, vk.mu_stride);
+                                                    vk.streamed ? 1 : 0, vk.row_stride, vk.mu_stride,
+                                                    vk.mmarec ? vk.mma_kt : 0);
         count_launch();
         STMG_CUDA(cudaGetLastError());
       };
@@ -800,7 +810,39 @@ namespace stmg
         nreal += teig.kind[k] == 1 ? 1 : 0;
       rowrec = streamed && teig.use && nd <= 32 && nreal == nt % 2 && !(e && e[0] == '0');
     }
-    if (rowrec)
+    {
+      // the tensor-core apply: BF16 storage, 3 or 4 time dofs (one brick word
+      // of four FP32 per node)
+      const char *e = std::getenv("STMG_VANKA_MMA");
+      mmarec        = rowrec && storage == STMG_BF16 && (nt == 3 || nt == 4) && !(e && e[0] == '0');
+    }
+    if (mmarec)
+      {
+        mma_kt     = nd <= 16 ? 16 : 32;
+        row_stride = mma_kt;
+        mu_off     = int(pad(nd * mma_kt * 2));
+        mu_stride  = 1;
+        rec_bytes  = int(pad(mu_off + nd * 4));
+        // eigenbasis with the complex pairs first, the real eigenvalue last
+        const int nr = nt % 2, np2 = nt - nr;
+        int       order[MAX_NT];
+        for (int k = 0; k < nt; ++k)
+          order[k] = k < np2 ? k + nr : k - np2; // new index k <- old index order[k]
+        teig_pf     = teig;
+        for (int k = 0; k < nt; ++k)
+          {
+            const int o       = order[k];
+            teig_pf.kind[k]   = teig.kind[o];
+            teig_pf.a[k]      = teig.a[o];
+            teig_pf.b[k]      = teig.b[o];
+            for (int j = 0; j < nt; ++j)
+              {
+                teig_pf.G[k * nt + j] = teig.G[o * nt + j]; // rows of G
+                teig_pf.S[j * nt + k] = teig.S[j * nt + o]; // columns of S
+              }
+          }
+      }
+    else if (rowrec)
       {
         row_stride = storage == STMG_F32 ? vk_row_stride<float>(int(nd)) : vk_row_stride<__nv_bfloat16>(int(nd));
         if (storage == STMG_F32)
@@ -843,6 +885,17 @@ namespace stmg
           {
             ok  = true;
             big = b;
+            // deeper record pipelines while two CTAs per SM still fit
+            if (rowrec)
+              while (stages < vanka_detail::VR_STAGES_MAX)
+                {
+                  ++stages;
+                  if (smem_bytes(shape) > (b ? 110 : 200) * 1024)
+                    {
+                      --stages;
+                      break;
+                    }
+                }
           }
       }
     if (!ok)

@@ -32,6 +32,28 @@ namespace stmg
     return sizeof(TS) == 4 ? (nd + 1 + 3) / 4 * 4 : (nd + 3) / 4 * 4;
   }
 
+  // Swizzled BF16 rows of the tensor-core apply: V by rows of KT entries (KT =
+  // 16 or 32, the mode/dof count padded for m16n8k16 tiles), the 16-byte
+  // chunks of row m permuted so that eight consecutive rows of one chunk
+  // column fall in eight different shared-memory bank groups (conflict-free
+  // ldmatrix); byte offset of entry (m, d) within the V block.
+  template <int KT>
+  struct MmaRows
+  {
+    static constexpr int CPR = KT / 8; // 16-byte chunks per row
+    static constexpr int RB  = 8 / CPR; // rows per swizzle step
+    __host__ __device__ static constexpr int
+    chunk(int m, int c)
+    {
+      return c ^ ((m / RB) & (CPR - 1));
+    }
+    __host__ __device__ static constexpr int
+    offset(int m, int d)
+    {
+      return m * KT * 2 + chunk(m, d / 8) * 16 + (d % 8) * 2;
+    }
+  };
+
   // Set by a Vanka apply kernel whose wait for a record copy gave up (mapped
   // host memory, read by Vanka::check_fault); 0 while all is well.
   int *vanka_fault_flag_device();
@@ -78,6 +100,15 @@ namespace stmg
     // mu values from mu_off (in the mu type)
     bool                  rowrec     = false;
     int                   row_stride = 0, mu_stride = 1;
+    // mmarec: BF16 row records in the swizzled layout of MmaRows<mma_kt>,
+    // applied by the tensor-core kernel (3 or 4 time dofs, nd <= 32); teig_pf
+    // is teig with complex pairs first (the kernel's lane layout)
+    bool                  mmarec = false;
+    // record stages of the row-record and tensor-core applies (3..5): as
+    // many colour phases in flight as two CTAs per SM leave room for
+    int                   stages = 3;
+    int                   mma_kt = 0;
+    TimeEig               teig_pf{};
     int                   colour_cells = 1;
     bool                  big = true;                // compile-time tile shape in use
     int                   shape[3] = {1, 1, 1};

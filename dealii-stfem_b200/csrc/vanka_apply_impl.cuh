@@ -692,12 +692,16 @@ namespace stmg
     // ------------------------------------------------- row-record apply
     // Record streaming by the bulk copy engine: one cp.async.bulk (global ->
     // this CTA's shared memory, no multicast) per colour phase, completing on
-    // an mbarrier. Every wait is bounded: after VR_WAIT_LIMIT polls the
+    // an mbarrier. Waiting threads sleep in mbarrier.try_wait (suspend-time
+    // hint) instead of polling, so they leave the issue slots to the warps
+    // that compute. Every wait is bounded: after VR_WAIT_NS of global time the
     // kernel sets the fault flag, waits (bounded) for the copies it issued and
     // returns.
-    constexpr int       VR_STAGES     = 3;         // record stages (colour phases in flight)
-    constexpr int       VR_WARPS      = 8;         // warps per CTA, a warp per cell
-    constexpr long long VR_WAIT_LIMIT = 1ll << 22; // polls of one barrier phase
+    constexpr int                VR_STAGES  = 3;             // fewest record stages (colour phases in flight - 1)
+    constexpr int                VR_STAGES_MAX = 5;          // most record stages
+    constexpr int                VR_WARPS   = 8;             // warps per CTA, a warp per cell
+    constexpr unsigned           VR_SUSPEND = 20000;         // ns a waiting thread may sleep per try_wait
+    constexpr unsigned long long VR_WAIT_NS = 2000000000ull; // give up a barrier phase after 2 s
 
     __device__ __forceinline__ unsigned
     smem_u32(const void *p)
@@ -723,23 +727,40 @@ namespace stmg
       asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
     }
 
+    __device__ __forceinline__ unsigned long long
+    global_ns()
+    {
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      return t;
+    }
+
+    // one try_wait: true if the phase of the given parity has completed; the
+    // thread may sleep up to VR_SUSPEND ns waiting for it
+    __device__ __forceinline__ bool
+    mbar_try_wait(unsigned bar, unsigned parity)
+    {
+      unsigned done;
+      asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                   "selp.u32 %0, 1, 0, p;\n}\n"
+                   : "=r"(done)
+                   : "r"(bar), "r"(parity), "r"(VR_SUSPEND)
+                   : "memory");
+      return done != 0;
+    }
+
     // true once the phase of the given parity has completed, false after
-    // VR_WAIT_LIMIT polls
+    // VR_WAIT_NS
     __device__ __forceinline__ bool
     mbar_wait(unsigned bar, unsigned parity)
     {
-      for (long long it = 0; it < VR_WAIT_LIMIT; ++it)
-        {
-          unsigned done;
-          asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                       "selp.u32 %0, 1, 0, p;\n}\n"
-                       : "=r"(done)
-                       : "r"(bar), "r"(parity)
-                       : "memory");
-          if (done)
-            return true;
-        }
-      return false;
+      if (mbar_try_wait(bar, parity))
+        return true;
+      const unsigned long long t0 = global_ns();
+      while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > VR_WAIT_NS)
+          return false;
+      return true;
     }
 
     // bytes (a multiple of 16, 16-byte aligned ends) global -> shared,
@@ -860,7 +881,7 @@ namespace stmg
     //    mode's solve is the scaling of mode_scale;
     //  * the time values of a node are added pairwise (FFMA2), the 27-term
     //    sums split into two chains.
-    template <int DIM, int P, typename TS, int NT, int TX, int TY, int TZ>
+    template <int DIM, int P, typename TS, int NT, int TX, int TY, int TZ, int STG>
     __global__ void __launch_bounds__(VR_WARPS * 32, 2)
     vanka_row_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeEig te,
                      const unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int cpc,
@@ -887,11 +908,11 @@ namespace stmg
       static_assert(S::E0 <= 32, "brick rows wider than a warp");
       extern __shared__ __align__(16) unsigned char vk_smem[];
       __shared__ int                             col_n[NC], col_pre[NC], col_cell[NC][CPC];
-      __shared__ __align__(8) unsigned long long bars[VR_STAGES];
+      __shared__ __align__(8) unsigned long long bars[STG];
       const int       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
       const int       lrow = lane / S::E0, lx = lane - lrow * S::E0;
       const long long stage_bytes = (long long)cpc * rec_bytes;
-      float          *bin0 = reinterpret_cast<float *>(vk_smem + VR_STAGES * stage_bytes);
+      float          *bin0 = reinterpret_cast<float *>(vk_smem + STG * stage_bytes);
       float          *bout = bin0 + 2 * S::NB * NTP;
       float          *wb   = bout + S::NB * NTP + warp * ND * NTP;
       const long long tcr  = (long long)tl.T[0] * tl.T[1] * tl.T[2];
@@ -928,7 +949,7 @@ namespace stmg
         }
       if (threadIdx.x == 0)
         {
-          for (int st = 0; st < VR_STAGES; ++st)
+          for (int st = 0; st < STG; ++st)
             mbar_init(smem_u32(&bars[st]), 1);
           asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         }
@@ -945,13 +966,13 @@ namespace stmg
             const int col  = k % NC;
             if (threadIdx.x == 0)
               {
-                const unsigned bar   = smem_u32(&bars[k % VR_STAGES]);
+                const unsigned bar   = smem_u32(&bars[k % STG]);
                 const unsigned bytes = unsigned(col_n[col]) * unsigned(rec_bytes);
                 if (bytes > 0)
                   {
                     fence_proxy_async_smem();
                     mbar_expect_tx(bar, bytes);
-                    bulk_copy_g2s(smem_u32(vk_smem + (k % VR_STAGES) * stage_bytes),
+                    bulk_copy_g2s(smem_u32(vk_smem + (k % STG) * stage_bytes),
                                   rec + (tile * tcr + col_pre[col]) * rec_bytes, bytes, bar);
                   }
                 else
@@ -983,19 +1004,19 @@ namespace stmg
       };
 
 #pragma unroll
-      for (int k = 0; k < VR_STAGES - 1; ++k)
+      for (int k = 0; k < STG - 1; ++k)
         issue(k);
 
       TileGeo tg{};
       int     k = 0;
       for (; k < phases; ++k)
         {
-          const bool arrived = mbar_wait(smem_u32(&bars[k % VR_STAGES]), unsigned(k / VR_STAGES) & 1u);
-          cp_async_wait<VR_STAGES - 2>();
+          const bool arrived = mbar_wait(smem_u32(&bars[k % STG]), unsigned(k / STG) & 1u);
+          cp_async_wait<STG - 2>();
           // phase k's records and brick visible; phase k-1 done (its stage free, its output adds made)
           if (__syncthreads_or(!arrived))
             break;
-          issue(k + VR_STAGES - 1);
+          issue(k + STG - 1);
 
           const int tile = blockIdx.x + (k / NC) * gridDim.x;
           const int col  = k % NC;
@@ -1014,7 +1035,7 @@ namespace stmg
               __syncthreads();
             }
           const int            n   = col_n[col];
-          const unsigned char *stg = vk_smem + (k % VR_STAGES) * stage_bytes;
+          const unsigned char *stg = vk_smem + (k % STG) * stage_bytes;
           for (int idx = warp; idx < n; idx += NW)
             {
               const int cl = col_cell[col][idx];
@@ -1146,9 +1167,444 @@ namespace stmg
           if (threadIdx.x == 0)
             {
               atomicExch(fault, 1);
-              const int last = min(phases, k + VR_STAGES - 1);
+              const int last = min(phases, k + STG - 1);
               for (int j = k; j < last; ++j)
-                mbar_wait(smem_u32(&bars[j % VR_STAGES]), unsigned(j / VR_STAGES) & 1u);
+                mbar_wait(smem_u32(&bars[j % STG]), unsigned(j / STG) & 1u);
+            }
+          __syncthreads();
+        }
+      cp_async_wait<0>();
+    }
+
+    // ---------------------------------------------- tensor-core apply
+    __device__ __forceinline__ void
+    ldsm_x4(unsigned addr, unsigned (&r)[4])
+    {
+      asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                   : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                   : "r"(addr));
+    }
+
+    __device__ __forceinline__ void
+    ldsm_x4_trans(unsigned addr, unsigned (&r)[4])
+    {
+      asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                   : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                   : "r"(addr));
+    }
+
+    // d += a b for one m16n8k16 tile, BF16 operands, FP32 accumulation
+    __device__ __forceinline__ void
+    mma_bf16_16816(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1)
+    {
+      asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                   "{%8, %9}, {%0, %1, %2, %3};\n"
+                   : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                   : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    }
+
+    // two floats as packed BF16 (lo in the low half), rounded to nearest
+    __device__ __forceinline__ unsigned
+    pack_bf16(float lo, float hi)
+    {
+      const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+      return *reinterpret_cast<const unsigned *>(&v);
+    }
+
+    // the rounding residuals x - bf16(x) of a packed pair, packed again
+    __device__ __forceinline__ unsigned
+    pack_bf16_residual(float lo, float hi, unsigned h)
+    {
+      return pack_bf16(lo - __uint_as_float(h << 16), hi - __uint_as_float(h & 0xffff0000u));
+    }
+
+    // Tensor-core apply for BF16 records (row records of MmaRows<KT>, 3 or 4
+    // time dofs): the streamed colour phases of the row-record apply with the
+    // two per-cell products on the tensor cores, one warp per cell:
+    //   pass 1  Y = V [x_hi | x_lo]  (m16n8k16, modes x 8 columns, K = dofs),
+    //           x = G x_in split into two BF16 parts per node when the tile's
+    //           brick arrives (x_hi + x_lo keeps ~16 significant bits), so
+    //           Y's column pairs t and t+4 add to the FP32-accurate V x;
+    //   scale   w = (mu Lambda + I)^{-1} y per mode (complex pairs first);
+    //   pass 2  out = V^T [w_hi | w_lo], added into the output brick;
+    // the tile's output is mapped back by S when it is written.
+    // Fragment layouts (PTX ISA, mma.m16n8k16 .bf16): lane = 4 g + t holds
+    // A(g, 2t..2t+1), A(g+8, ..), A(g, 2t+8..), A(g+8, 2t+8..); B(2t..2t+1, g),
+    // B(2t+8..2t+9, g); C(g, 2t..2t+1), C(g+8, 2t..2t+1).
+    template <int DIM, int P, int NT, int TX, int TY, int TZ, int STG>
+    __global__ void __launch_bounds__(VR_WARPS * 32, 2)
+    vanka_mma_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeEig te,
+                     const unsigned char *__restrict__ rec, int rec_bytes, int mu_off, int cpc,
+                     const float *__restrict__ src, float *__restrict__ dst, float *__restrict__ shell,
+                     const OutMode<float> om, int *__restrict__ fault)
+    {
+      using S           = TileShape<DIM, P, TX, TY, TZ>;
+      using TV          = TimeVec<NT>;
+      constexpr int ND  = S::ND;
+      constexpr int NTP = 4;
+      constexpr int KT  = ND <= 16 ? 16 : 32; // padded modes / dofs
+      constexpr int NKT = KT / 16;            // m16n8k16 tiles per dimension
+      constexpr int NR  = NT % 2;             // one real eigenvalue for odd n_t, last
+      constexpr int NPT = NT - NR;            // time dofs in complex pairs
+      constexpr int NC  = 1 << DIM;
+      constexpr int CPC = ((TX + 1) / 2) * ((TY + 1) / 2) * (DIM == 3 ? (TZ + 1) / 2 : 1);
+      constexpr int NW  = VR_WARPS;
+      constexpr int RPW = 32 / S::E0;
+      constexpr int ROWS = NT * S::E1 * S::E2;
+      using MR          = MmaRows<KT>;
+      static_assert(TV::NTP == 4, "tensor-core apply: 3 or 4 time dofs");
+      static_assert(ND <= 32, "tensor-core apply: at most 32 dofs per cell");
+      extern __shared__ __align__(16) unsigned char vk_smem[];
+      __shared__ int                             col_n[NC], col_pre[NC], col_cell[NC][CPC];
+      __shared__ __align__(8) unsigned long long bars[STG];
+      const int       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const int       g = lane >> 2, t = lane & 3;
+      const int       lrow = lane / S::E0, lx = lane - lrow * S::E0;
+      const long long stage_bytes = (long long)cpc * rec_bytes;
+      float          *bin0 = reinterpret_cast<float *>(vk_smem + STG * stage_bytes);
+      float          *bout = bin0 + 2 * S::NB * NTP;
+      unsigned char  *wbw  = reinterpret_cast<unsigned char *>(bout + S::NB * NTP) + warp * 32 * 16; // [32 modes][8 bf16]
+      unsigned char  *zero = reinterpret_cast<unsigned char *>(bout + S::NB * NTP) + NW * 32 * 16;  // 128 zero bytes
+      const long long tcr  = (long long)tl.T[0] * tl.T[1] * tl.T[2];
+      const int       my_tiles = int(blockIdx.x) < tl.n_tiles ? int((tl.n_tiles - 1 - blockIdx.x) / gridDim.x) + 1 : 0;
+      const int       phases   = my_tiles * NC;
+
+      // brick offsets (cell-relative) of this lane's dofs: pass-1 B rows
+      // d = 16 kt + 2t + {0, 1, 8, 9}; output rows d = g + 8 i
+      int  boff[NKT][4], ooff[NKT * 2];
+      bool bok[NKT][4], ook[NKT * 2];
+#pragma unroll
+      for (int kt = 0; kt < NKT; ++kt)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          {
+            const int d  = 16 * kt + 2 * t + (q & 1) + 8 * (q >> 1);
+            bok[kt][q]   = d < ND;
+            boff[kt][q]  = S::offset(d < ND ? d : 0);
+          }
+#pragma unroll
+      for (int i = 0; i < NKT * 2; ++i)
+        {
+          const int d = g + 8 * i;
+          ook[i]      = d < ND;
+          ooff[i]     = S::offset(d < ND ? d : 0);
+        }
+
+      if (threadIdx.x < NC)
+        {
+          const int col = threadIdx.x;
+          int       cnt[3], n = 1, pre = 0;
+          for (int c = 0; c <= col; ++c)
+            {
+              int nc = 1;
+#pragma unroll
+              for (int d = 0; d < 3; ++d)
+                {
+                  const int o = (c >> d) & 1;
+                  cnt[d]      = d < DIM ? (tl.T[d] - o + 1) / 2 : (o ? 0 : 1);
+                  nc *= cnt[d];
+                }
+              if (c < col)
+                pre += nc;
+              else
+                n = nc;
+            }
+          col_n[col]   = n;
+          col_pre[col] = pre;
+          for (int idx = 0; idx < n && idx < CPC; ++idx)
+            {
+              const int ix = idx % cnt[0], iy = (idx / cnt[0]) % cnt[1], iz = idx / (cnt[0] * cnt[1]);
+              const int cx = 2 * ix + (col & 1), cy = 2 * iy + ((col >> 1) & 1), cz = 2 * iz + ((col >> 2) & 1);
+              col_cell[col][idx] = cx | (cy << 8) | (cz << 16);
+            }
+        }
+      if (threadIdx.x == 0)
+        {
+          for (int st = 0; st < STG; ++st)
+            mbar_init(smem_u32(&bars[st]), 1);
+          asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+      for (int idx = threadIdx.x; idx < S::NB * NTP; idx += blockDim.x)
+        bout[idx] = 0.0f;
+      // the per-warp w buffers (rows of modes >= nd stay zero) and the zero block
+      for (int idx = threadIdx.x; idx < (NW * 32 * 16 + 128) / 4; idx += blockDim.x)
+        reinterpret_cast<unsigned *>(bout + S::NB * NTP)[idx] = 0u;
+      __syncthreads();
+
+      auto issue = [&](int k) {
+        if (k < phases)
+          {
+            const int tile = blockIdx.x + (k / NC) * gridDim.x;
+            const int col  = k % NC;
+            if (threadIdx.x == 0)
+              {
+                const unsigned bar   = smem_u32(&bars[k % STG]);
+                const unsigned bytes = unsigned(col_n[col]) * unsigned(rec_bytes);
+                if (bytes > 0)
+                  {
+                    fence_proxy_async_smem();
+                    mbar_expect_tx(bar, bytes);
+                    bulk_copy_g2s(smem_u32(vk_smem + (k % STG) * stage_bytes),
+                                  rec + (tile * tcr + col_pre[col]) * rec_bytes, bytes, bar);
+                  }
+                else
+                  mbar_arrive(bar);
+              }
+            if (col == 0)
+              {
+                const TileGeo tg  = tile_geo<DIM, P>(m, tl, tile);
+                float        *bi  = bin0 + ((k / NC) & 1) * S::NB * NTP;
+                const int     gx  = tg.c0[0] * P + lx;
+                const bool    okx = lx < tg.e[0] && gx > 0 && gx < m.nn[0] - 1;
+                for (int rb = warp * RPW; rb < ROWS; rb += NW * RPW)
+                  {
+                    const int row = rb + lrow;
+                    if (lrow >= RPW || row >= ROWS)
+                      continue;
+                    const int i = row / (S::E1 * S::E2), rem = row - i * (S::E1 * S::E2);
+                    const int bz = rem / S::E1, by = rem - bz * S::E1;
+                    const int gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
+                    bool      ok = okx && by < tg.e[1] && bz < tg.e[2] && gy > 0 && gy < m.nn[1] - 1;
+                    if (DIM == 3)
+                      ok = ok && gz > 0 && gz < m.nn[2] - 1;
+                    const float *gp = ok ? src + i * m.N + gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz) : src;
+                    cp_async_small<4>(bi + ((bz * S::E1 + by) * S::E0 + lx) * NTP + i, gp, ok);
+                  }
+              }
+          }
+        cp_async_commit();
+      };
+
+#pragma unroll
+      for (int k = 0; k < STG - 1; ++k)
+        issue(k);
+
+      TileGeo tg{};
+      int     k = 0;
+      for (; k < phases; ++k)
+        {
+          const bool arrived = mbar_wait(smem_u32(&bars[k % STG]), unsigned(k / STG) & 1u);
+          cp_async_wait<STG - 2>();
+          if (__syncthreads_or(!arrived))
+            break;
+          issue(k + STG - 1);
+
+          const int tile = blockIdx.x + (k / NC) * gridDim.x;
+          const int col  = k % NC;
+          float    *bi   = bin0 + ((k / NC) & 1) * S::NB * NTP;
+          if (col == 0)
+            {
+              tg = tile_geo<DIM, P>(m, tl, tile);
+              // the tile's input in the eigenbasis, split in BF16 parts: per
+              // node 8 BF16 (G x rounded, then the rounding residuals) in
+              // place of the node's four FP32 values
+              for (int nd = threadIdx.x; nd < S::NB; nd += blockDim.x)
+                {
+                  float v[NT];
+                  TV::load(bi + nd * NTP, v);
+                  time_map<NT>(te.G, v);
+                  float w4[4] = {v[0], NT > 1 ? v[1] : 0.0f, NT > 2 ? v[2] : 0.0f, NT > 3 ? v[NT - 1] : 0.0f};
+                  if (NT == 3)
+                    w4[3] = 0.0f;
+                  const unsigned h0 = pack_bf16(w4[0], w4[1]), h1 = pack_bf16(w4[2], w4[3]);
+                  const unsigned l0 = pack_bf16_residual(w4[0], w4[1], h0), l1 = pack_bf16_residual(w4[2], w4[3], h1);
+                  *reinterpret_cast<uint4 *>(bi + nd * NTP) = make_uint4(h0, h1, l0, l1);
+                }
+              __syncthreads();
+            }
+          const int            n   = col_n[col];
+          const unsigned char *stg = vk_smem + (k % STG) * stage_bytes;
+          const unsigned short *xb = reinterpret_cast<const unsigned short *>(bi); // 8 BF16 per node
+          for (int idx = warp; idx < n; idx += NW)
+            {
+              const int cl = col_cell[col][idx];
+              const int cx = cl & 255, cy = (cl >> 8) & 255, cz = cl >> 16;
+              if (cx >= tg.tc[0] || cy >= tg.tc[1] || cz >= tg.tc[2])
+                continue;
+              const unsigned char *r     = stg + idx * rec_bytes;
+              const unsigned       rs    = smem_u32(r), zs = smem_u32(zero);
+              const int            bbase = cx * P + S::E0 * (cy * P + S::E1 * (cz * P));
+
+              // pass 1: Y = V X, modes x (4 hi + 4 lo columns)
+              float y[NKT][4];
+#pragma unroll
+              for (int mt = 0; mt < NKT; ++mt)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                  y[mt][q] = 0.0f;
+#pragma unroll
+              for (int kt = 0; kt < NKT; ++kt)
+                {
+                  // B: X(d, g) for d = 16 kt + 2t + {0, 1, 8, 9}
+                  unsigned short xv[4];
+#pragma unroll
+                  for (int q = 0; q < 4; ++q)
+                    xv[q] = bok[kt][q] ? xb[(bbase + boff[kt][q]) * 8 + g] : (unsigned short)0;
+                  const unsigned b0 = unsigned(xv[0]) | (unsigned(xv[1]) << 16);
+                  const unsigned b1 = unsigned(xv[2]) | (unsigned(xv[3]) << 16);
+#pragma unroll
+                  for (int mt = 0; mt < NKT; ++mt)
+                    {
+                      // A: V rows 16 mt + 8 (j & 1) + r, dof chunk 2 kt + (j >> 1)
+                      const int j = lane >> 3, rr = lane & 7;
+                      const int mrow = 16 * mt + 8 * (j & 1) + rr;
+                      const unsigned ad = mrow < ND ? rs + unsigned(MR::offset(mrow, 16 * kt + 8 * (j >> 1)))
+                                                    : zs + unsigned(16 * rr);
+                      unsigned a[4];
+                      ldsm_x4(ad, a);
+                      mma_bf16_16816(y[mt], a, b0, b1);
+                    }
+                }
+              // columns t and t + 4 (lanes t and t ^ 2) add up: V x for times
+              // 2 (t & 1), 2 (t & 1) + 1 of modes 16 mt + g (+ 8)
+              const int tau = 2 * (t & 1);
+#pragma unroll
+              for (int mt = 0; mt < NKT; ++mt)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                  y[mt][q] += __shfl_xor_sync(0xffffffffu, y[mt][q], 2);
+              // time solves: w = (mu Lambda + I)^{-1} y in the pair (tau, tau + 1)
+              const float *mu = reinterpret_cast<const float *>(r + mu_off);
+#pragma unroll
+              for (int mt = 0; mt < NKT; ++mt)
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh)
+                  {
+                    const int   mode = 16 * mt + g + 8 * hh;
+                    const float mm   = mu[mode < ND ? mode : 0];
+                    float       u = y[mt][2 * hh], v = y[mt][2 * hh + 1];
+                    if (tau + 1 < NPT)
+                      {
+                        const float d = fmaf(mm, te.a[tau], 1.0f), e = mm * te.b[tau];
+                        const float inv = rcp_approx(fmaf(d, d, e * e));
+                        const float wu = inv * fmaf(d, u, -e * v), wv = inv * fmaf(e, u, d * v);
+                        u = wu;
+                        v = wv;
+                      }
+                    else if (tau < NT)
+                      {
+                        u *= rcp_approx(fmaf(mm, te.a[tau], 1.0f));
+                        v = 0.0f;
+                      }
+                    else
+                      u = v = 0.0f;
+                    // lanes t < 2 store the BF16 parts, lanes t >= 2 the residuals
+                    if (mode < ND)
+                      {
+                        const unsigned h = pack_bf16(u, v);
+                        const unsigned o = t < 2 ? h : pack_bf16_residual(u, v, h);
+                        *reinterpret_cast<unsigned *>(wbw + mode * 16 + (t < 2 ? 0 : 8) + 2 * tau) = o;
+                      }
+                  }
+              __syncwarp();
+
+              // pass 2: out = V^T W, dofs x (4 hi + 4 lo columns)
+              float o[NKT][4];
+#pragma unroll
+              for (int mt = 0; mt < NKT; ++mt)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                  o[mt][q] = 0.0f;
+              const unsigned short *wb16 = reinterpret_cast<const unsigned short *>(wbw);
+#pragma unroll
+              for (int kt = 0; kt < NKT; ++kt)
+                {
+                  // B: W(mode, g) for mode = 16 kt + 2t + {0, 1, 8, 9}
+                  const int      m0 = 16 * kt + 2 * t;
+                  const unsigned b0 = unsigned(wb16[m0 * 8 + g]) | (unsigned(wb16[(m0 + 1) * 8 + g]) << 16);
+                  const unsigned b1 = unsigned(wb16[(m0 + 8) * 8 + g]) | (unsigned(wb16[(m0 + 9) * 8 + g]) << 16);
+#pragma unroll
+                  for (int mt = 0; mt < NKT; ++mt)
+                    {
+                      // A = V^T: rows (modes) 16 kt + 8 (j >> 1) + r of V, dof chunk 2 mt + (j & 1), transposed
+                      const int j = lane >> 3, rr = lane & 7;
+                      const int mrow = 16 * kt + 8 * (j >> 1) + rr;
+                      const unsigned ad = mrow < ND ? rs + unsigned(MR::offset(mrow, 16 * mt + 8 * (j & 1)))
+                                                    : zs + unsigned(16 * rr);
+                      unsigned a[4];
+                      ldsm_x4_trans(ad, a);
+                      mma_bf16_16816(o[mt], a, b0, b1);
+                    }
+                }
+#pragma unroll
+              for (int mt = 0; mt < NKT; ++mt)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                  o[mt][q] += __shfl_xor_sync(0xffffffffu, o[mt][q], 2);
+              if (t < 2)
+                {
+#pragma unroll
+                  for (int mt = 0; mt < NKT; ++mt)
+#pragma unroll
+                    for (int hh = 0; hh < 2; ++hh)
+                      {
+                        const int i = 2 * mt + hh; // dof g + 8 i
+                        if (!ook[i])
+                          continue;
+                        float2 *ob  = reinterpret_cast<float2 *>(bout + (bbase + ooff[i]) * NTP + tau);
+                        float2  cur = *ob;
+                        cur.x += o[mt][2 * hh];
+                        cur.y += o[mt][2 * hh + 1];
+                        *ob = cur;
+                      }
+                }
+              __syncwarp();
+            }
+          if (col == NC - 1)
+            {
+              __syncthreads();
+              const int  gx  = tg.c0[0] * P + lx;
+              const int  vx  = (gx % P == 0) ? 2 : 1;
+              const bool inx = lx > 0 && lx < tg.e[0] - 1;
+              for (int rb = warp * RPW; rb < S::E1 * S::E2; rb += NW * RPW)
+                {
+                  const int row = rb + lrow;
+                  if (lrow >= RPW || row >= S::E1 * S::E2 || lx >= tg.e[0])
+                    continue;
+                  const int bz = row / S::E1, by = row - bz * S::E1;
+                  if (by >= tg.e[1] || bz >= tg.e[2])
+                    continue;
+                  bool inte = inx && by > 0 && by < tg.e[1] - 1;
+                  if (DIM == 3)
+                    inte = inte && bz > 0 && bz < tg.e[2] - 1;
+                  const int gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
+                  int       v  = vx * ((gy % P == 0) ? 2 : 1);
+                  if (DIM == 3)
+                    v *= (gz % P == 0) ? 2 : 1;
+                  const float w = v == 1 ? 1.0f : (v == 2 ? 0.5f : (v == 4 ? 0.25f : 0.125f));
+                  float       ov[NT];
+                  TV::load(bout + ((bz * S::E1 + by) * S::E0 + lx) * NTP, ov);
+                  time_map<NT>(te.S, ov);
+                  long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+                  if (inte)
+#pragma unroll
+                    for (int jt = 0; jt < NT; ++jt, gi += m.N)
+                      om.write(dst, gi, ov[jt] * w);
+                  else if (tl.n_tiles == 1)
+#pragma unroll
+                    for (int jt = 0; jt < NT; ++jt, gi += m.N)
+                      om.write_constrained(dst, gi);
+                  else
+                    {
+                      float *sj = shell + (long long)tile * NT * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz);
+#pragma unroll
+                      for (int jt = 0; jt < NT; ++jt, sj += tl.tile_stride)
+                        *sj = ov[jt];
+                    }
+                }
+              __syncthreads();
+              for (int idx = threadIdx.x; idx < S::NB * NTP; idx += blockDim.x)
+                bout[idx] = 0.0f;
+            }
+        }
+      if (k < phases)
+        {
+          if (threadIdx.x == 0)
+            {
+              atomicExch(fault, 1);
+              const int last = min(phases, k + STG - 1);
+              for (int j = k; j < last; ++j)
+                mbar_wait(smem_u32(&bars[j % STG]), unsigned(j / STG) & 1u);
             }
           __syncthreads();
         }
@@ -1193,7 +1649,9 @@ namespace stmg
           const MeshView   &m    = vk.mesh->v;
           const Tiling     &tl   = vk.tiling;
           const std::size_t smem = vk.smem_bytes(vk.shape);
-          auto              kern = vanka_row_kernel<DIM, P, TS, NT, Sh::TX, Sh::TY, Sh::TZ>;
+          auto kern = vk.stages >= 5 ? vanka_row_kernel<DIM, P, TS, NT, Sh::TX, Sh::TY, Sh::TZ, 5>
+                    : vk.stages == 4 ? vanka_row_kernel<DIM, P, TS, NT, Sh::TX, Sh::TY, Sh::TZ, 4>
+                                     : vanka_row_kernel<DIM, P, TS, NT, Sh::TX, Sh::TY, Sh::TZ, 3>;
           const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), VR_WARPS * 32, smem, tl.n_tiles);
           kern<<<grid, VR_WARPS * 32, smem, s>>>(m, tl, vk.teig, vk.V.ptr, vk.rec_bytes, vk.mu_off, vk.colour_cells, src,
                                                  dst, reinterpret_cast<float *>(vk.shell.ptr), om,
@@ -1207,10 +1665,45 @@ namespace stmg
         throw Error(STMG_ERR_UNSUPPORTED, "vanka: row records need at most 32 dofs per cell");
     }
 
+    template <int DIM, int P, int NT, bool BIG>
+    void
+    launch_mma(const Vanka &vk, const float *src, float *dst, const OutMode<float> &om, cudaStream_t s)
+    {
+      using Sh = VkShape<DIM, P, BIG>;
+      if constexpr (Tens<P + 1, DIM>::ND <= 32 && (NT == 3 || NT == 4))
+        {
+          const MeshView   &m    = vk.mesh->v;
+          const Tiling     &tl   = vk.tiling;
+          const std::size_t smem = vk.smem_bytes(vk.shape);
+          auto kern = vk.stages >= 5 ? vanka_mma_kernel<DIM, P, NT, Sh::TX, Sh::TY, Sh::TZ, 5>
+                    : vk.stages == 4 ? vanka_mma_kernel<DIM, P, NT, Sh::TX, Sh::TY, Sh::TZ, 4>
+                                     : vanka_mma_kernel<DIM, P, NT, Sh::TX, Sh::TY, Sh::TZ, 3>;
+          const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), VR_WARPS * 32, smem, tl.n_tiles);
+          kern<<<grid, VR_WARPS * 32, smem, s>>>(m, tl, vk.teig_pf, vk.V.ptr, vk.rec_bytes, vk.mu_off, vk.colour_cells,
+                                                 src, dst, reinterpret_cast<float *>(vk.shell.ptr), om,
+                                                 vanka_fault_flag_device());
+          count_launch();
+          STMG_CUDA(cudaGetLastError());
+          if (tl.n_tiles > 1)
+            launch_plane_fixup<DIM, float, true>(m, tl, vk.nt, reinterpret_cast<float *>(vk.shell.ptr), dst, om, s);
+        }
+      else
+        throw Error(STMG_ERR_UNSUPPORTED, "vanka: the tensor-core apply needs 3 or 4 time dofs and 32 dofs per cell");
+    }
+
     template <int DIM, int P, typename TS, int NT>
     void
     launch_stream_nt(const Vanka &vk, const float *src, float *dst, const OutMode<float> &om, cudaStream_t s)
     {
+      if constexpr (std::is_same_v<TS, __nv_bfloat16>)
+        if (vk.mmarec)
+          {
+            if (vk.big)
+              launch_mma<DIM, P, NT, true>(vk, src, dst, om, s);
+            else
+              launch_mma<DIM, P, NT, false>(vk, src, dst, om, s);
+            return;
+          }
       if (vk.rowrec)
         {
           if (vk.big)
