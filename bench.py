@@ -105,16 +105,17 @@ class ClockSampler:
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one
-# finest-level FP32 Vanka apply, from an ncu capture of the same kernel on
+# finest-level Vanka apply kernel, from ncu captures of the same kernels on
 # 64^3 Q2 cells with n_t = 4 (the records exceed L2 there, and the traffic
 # grows with the cell count): python bench.py --kernels-only vanka_apply
-# --refine 6 under ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum.
-VANKA_TRAFFIC_PER_CELL = 3523.76
+# --refine 6 [--vanka-storage bf16] under ncu --set full (vanka_row_kernel
+# with FP32 records, vanka_mma_kernel with BF16 records).
+VANKA_TRAFFIC_PER_CELL = {"f32": 3508.62, "bf16": 2301.93}
 
 
-def vanka_traffic(refine):
+def vanka_traffic(refine, storage="f32"):
     """DRAM bytes of one finest-level Vanka apply on (2^refine)^3 cells."""
-    return VANKA_TRAFFIC_PER_CELL * (1 << refine) ** 3
+    return VANKA_TRAFFIC_PER_CELL[storage] * (1 << refine) ** 3
 
 
 def peaks():
@@ -401,7 +402,7 @@ def run_ours(args):
 
     kr = kernel_roofline(stmg, torch, w, kappa, hbm, bf16=bf16)
     dom = max(kr, key=lambda k: kr[k]["ms"])
-    traffic = vanka_traffic(w["refine"]) if dom == "vanka_apply" else None
+    traffic = vanka_traffic(w["refine"], args.vanka_storage) if dom == "vanka_apply" else None
     roof = dict(kernel=dom, bound="hbm", achieved=kr[dom]["achieved"], peak=hbm, unit="GB/s",
                 frac=kr[dom]["frac"], traffic=traffic, peak_kind=hbm_kind,
                 kernels={k: dict(ms=v["ms"], algorithmic_bytes=v["bytes"], achieved_gbs=v["achieved"], frac=v["frac"])
