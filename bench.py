@@ -261,7 +261,9 @@ def kernel_roofline(stmg, torch, w, kappa, hbm, only=None, fp64=False, bf16=Fals
     events on the launching stream; algorithmic bytes per launch:
       operator: 2 n_t N 4 (read src, write dst) + cells 4 (coefficient)
       Vanka:    cells (nd^2 s + nd 4) (eigenvectors in the storage type s,
-                eigenvalues) + 2 n_t N 4."""
+                eigenvalues) + 2 n_t N 4
+      h-transfer to the next coarser mesh (N_c nodes), FP32:
+                prolongate-add n_t (N_c + 2 N) 4, restrict-add n_t (N + 2 N_c) 4."""
     n = 1 << w["refine"]
     mesh = stmg.Mesh(3, (n, n, n), 2, coeff=kappa)
     A, B, _, _, _ = stmg.time_weights(stmg.DG, 3, w["tau"], 1, stmg.HEAT)
@@ -273,10 +275,22 @@ def kernel_roofline(stmg, torch, w, kappa, hbm, only=None, fp64=False, bf16=Fals
     op = stmg.Operator(mesh, A, B, dtype=stmg.F64 if fp64 else stmg.F32) if only in (None, "st_apply") else None
     vk = stmg.Vanka(mesh, A, B, compute=stmg.F32, storage=stmg.BF16 if bf16 else stmg.F32) \
         if only in (None, "vanka_apply") else None
+    tr = xc = yc = None
+    Nc = (n + 1) ** 3
+    if only in (None, "h_transfer"):
+        coarse = stmg.Mesh(3, (n // 2,) * 3, 2)
+        tr = stmg.Transfer(mesh, coarse, nt, dtype=stmg.F32)
+        xc = torch.randn(nt * Nc, device="cuda", dtype=torch.float32)
+        yc = torch.zeros_like(xc)
+        x32 = x.float()
+        y32 = torch.zeros_like(x32)
     sz = 8 if fp64 else 4
     for name, fn, nbytes in (("st_apply", lambda: op.vmult(y, x), 2 * nt * N * sz + w["cells"] * sz),
-                             ("vanka_apply", lambda: vk.vmult(y, x), w["cells"] * vanka_record_bytes(bf16) + 2 * nt * N * 4)):
-        if only is not None and name != only:
+                             ("vanka_apply", lambda: vk.vmult(y, x), w["cells"] * vanka_record_bytes(bf16) + 2 * nt * N * 4),
+                             ("h_prolongate", lambda: tr.prolongate_add(y32, xc), nt * (Nc + 2 * N) * 4),
+                             ("h_restrict", lambda: tr.restrict_add(yc, x32), nt * (N + 2 * Nc) * 4)):
+        kind = "h_transfer" if name.startswith("h_") else name
+        if only is not None and kind != only:
             continue
         for _ in range(3):
             fn()
@@ -291,7 +305,7 @@ def kernel_roofline(stmg, torch, w, kappa, hbm, only=None, fp64=False, bf16=Fals
         t = e0.elapsed_time(e1) / 1e3 / reps
         gbs = nbytes / t / 1e9
         out[name] = dict(ms=t * 1e3, bytes=nbytes, achieved=gbs, frac=gbs / hbm)
-    del op, vk, mesh
+    del op, vk, tr, xc, yc, mesh
     torch.cuda.empty_cache()
     return out
 
@@ -628,7 +642,7 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the per-slab comparison of the FP32-MG and FP64-MG solutions with a converged "
                          "FP64 solve")
-    ap.add_argument("--kernels-only", choices=["all", "st_apply", "st_apply64", "vanka_apply"], default=None,
+    ap.add_argument("--kernels-only", choices=["all", "st_apply", "st_apply64", "vanka_apply", "h_transfer"], default=None,
                     help="only time the finest-level operator (FP32 or FP64) and/or Vanka apply in isolation "
                          "(profiling)")
     ap.add_argument("--adjoint", action="store_true", help="time the adjoint gradient configuration")

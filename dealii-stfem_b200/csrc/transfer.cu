@@ -52,106 +52,131 @@ namespace stmg
                       : (P <= 2 ? 32 / (2 * P) : (P == 3 ? 5 : (P == 4 ? 4 : 3)));
     }
 
-    // Prolongation dst_f += P src_c, one CTA per tile of C^dim coarse cells:
-    // the coarse block (P C + 1 nodes per direction, Dirichlet nodes zero) is
-    // interpolated direction by direction in shared memory (x, then y, then
-    // z) and the fine nodes the tile owns are added to dst (Dirichlet nodes
-    // skipped). Fine nodes [2PC t, 2PC (t+1)) belong to tile t; the last fine
-    // node to the last tile.
+    // dst[off] += v for the items of one pass of a CTA: each thread takes
+    // items threadIdx.x + blockDim.x k, KB at a time, and has the KB loads of
+    // dst in flight before it stores (one read-add-write per item, as in a
+    // plain loop, without a global-memory round trip per item)
+    template <int KB, typename T, typename Item>
+    __device__ __forceinline__ void
+    batched_add(int n, T *__restrict__ dst, const Item &item)
+    {
+      for (int base = threadIdx.x; base < n; base += KB * blockDim.x)
+        {
+          long long off[KB];
+          T         v[KB], old[KB];
+          bool      ok[KB];
+#pragma unroll
+          for (int k = 0; k < KB; ++k)
+            {
+              const int i = base + k * blockDim.x;
+              ok[k]       = i < n && item(i, off[k], v[k]);
+            }
+#pragma unroll
+          for (int k = 0; k < KB; ++k)
+            old[k] = ok[k] ? dst[off[k]] : T(0);
+#pragma unroll
+          for (int k = 0; k < KB; ++k)
+            if (ok[k])
+              dst[off[k]] = old[k] + v[k];
+        }
+    }
+
+    // Prolongation dst_f += P src_c, one CTA per tile of C^dim coarse cells
+    // and time dof (blockIdx.y): the coarse block (P C + 1 nodes per
+    // direction, Dirichlet nodes zero) is interpolated direction by direction
+    // in shared memory (x, then y, then z) and the fine nodes the tile owns
+    // are added to dst (Dirichlet nodes skipped). Fine nodes
+    // [2PC t, 2PC (t+1)) belong to tile t; the last fine node to the last
+    // tile.
     template <int DIM, int P, int C, typename T>
     __global__ void __launch_bounds__(256)
-    h_prolongate_tiled(const MeshView fm, const MeshView cm, int nt, const __grid_constant__ HWeights<T> W,
+    h_prolongate_tiled(const MeshView fm, const MeshView cm, const __grid_constant__ HWeights<T> W,
                        const T *__restrict__ src, T *__restrict__ dst)
     {
       constexpr int LC = P * C + 1, LF = 2 * P * C + 1;
       constexpr int NZC = DIM == 3 ? LC : 1, NZF = DIM == 3 ? LF : 1;
       __shared__ T sc[NZC * LC * LC], s1[NZC * LC * LF], s2[NZC * LF * LF];
       const int ntx = (cm.n[0] + C - 1) / C, nty = (cm.n[1] + C - 1) / C;
-      const int tile = blockIdx.x;
+      const int tile = blockIdx.x, j = blockIdx.y;
       const int t0 = tile % ntx, t1 = (tile / ntx) % nty, t2 = DIM == 3 ? tile / (ntx * nty) : 0;
       const int q0[3] = {t0 * C * P, t1 * C * P, t2 * C * P};        // first coarse node
       const int f0[3] = {2 * t0 * C * P, 2 * t1 * C * P, 2 * t2 * C * P}; // first fine node
-      for (int j = 0; j < nt; ++j)
+      for (int i = threadIdx.x; i < NZC * LC * LC; i += blockDim.x)
         {
-          for (int i = threadIdx.x; i < NZC * LC * LC; i += blockDim.x)
-            {
-              const int x = i % LC, y = (i / LC) % LC, z = i / (LC * LC);
-              const int g[3] = {q0[0] + x, q0[1] + y, DIM == 3 ? q0[2] + z : 0};
-              bool      ok   = g[0] < cm.nn[0] && g[1] < cm.nn[1] && (DIM < 3 || g[2] < cm.nn[2]);
-              ok             = ok && !is_boundary_node(cm, g[0], g[1], g[2]);
-              cp_async_small<sizeof(T)>(sc + i,
-                                        ok ? src + j * cm.N + g[0] + (long long)cm.nn[0] * (g[1] + (long long)cm.nn[1] * g[2])
-                                           : src,
-                                        ok);
-            }
-          cp_async_commit();
-          cp_async_wait<0>();
-          __syncthreads();
-          // x: sc[z][y][cx] -> s1[z][y][fx]
-          for (int i = threadIdx.x; i < NZC * LC * LF; i += blockDim.x)
-            {
-              const int fx = i % LF, r = i / LF;
-              const int cc = min(fx / (2 * P), C - 1), t = fx - 2 * P * cc;
-              const T  *in = sc + r * LC + P * cc;
-              T         v  = T(0);
-#pragma unroll
-              for (int b = 0; b <= P; ++b)
-                v += W.w[t][b] * in[b];
-              s1[i] = v;
-            }
-          __syncthreads();
-          // y: s1[z][cy][fx] -> s2[z][fy][fx]
-          for (int i = threadIdx.x; i < NZC * LF * LF; i += blockDim.x)
-            {
-              const int fx = i % LF, fy = (i / LF) % LF, z = i / (LF * LF);
-              const int cc = min(fy / (2 * P), C - 1), t = fy - 2 * P * cc;
-              const T  *in = s1 + (z * LC + P * cc) * LF + fx;
-              T         v  = T(0);
-#pragma unroll
-              for (int b = 0; b <= P; ++b)
-                v += W.w[t][b] * in[b * LF];
-              s2[i] = v;
-            }
-          __syncthreads();
-          // z (3-D): s2[cz][fy][fx] -> fine, added to dst
-          for (int i = threadIdx.x; i < NZF * LF * LF; i += blockDim.x)
-            {
-              const int fx = i % LF, fy = (i / LF) % LF, fz = i / (LF * LF);
-              const int g[3] = {f0[0] + fx, f0[1] + fy, DIM == 3 ? f0[2] + fz : 0};
-              // owned: below the next tile's first node, or the mesh's last node
-              bool own = (fx < LF - 1 || g[0] == fm.nn[0] - 1) && (fy < LF - 1 || g[1] == fm.nn[1] - 1);
-              if (DIM == 3)
-                own = own && (fz < LF - 1 || g[2] == fm.nn[2] - 1);
-              own = own && g[0] < fm.nn[0] && g[1] < fm.nn[1] && (DIM < 3 || g[2] < fm.nn[2]);
-              if (!own || is_boundary_node(fm, g[0], g[1], g[2]))
-                continue;
-              T v;
-              if constexpr (DIM == 3)
-                {
-                  const int cc = min(fz / (2 * P), C - 1), t = fz - 2 * P * cc;
-                  const T  *in = s2 + (P * cc) * LF * LF + fy * LF + fx;
-                  v            = T(0);
-#pragma unroll
-                  for (int b = 0; b <= P; ++b)
-                    v += W.w[t][b] * in[b * LF * LF];
-                }
-              else
-                v = s2[i];
-              dst[j * fm.N + g[0] + (long long)fm.nn[0] * (g[1] + (long long)fm.nn[1] * g[2])] += v;
-            }
-          __syncthreads();
+          const int x = i % LC, y = (i / LC) % LC, z = i / (LC * LC);
+          const int g[3] = {q0[0] + x, q0[1] + y, DIM == 3 ? q0[2] + z : 0};
+          bool      ok   = g[0] < cm.nn[0] && g[1] < cm.nn[1] && (DIM < 3 || g[2] < cm.nn[2]);
+          ok             = ok && !is_boundary_node(cm, g[0], g[1], g[2]);
+          cp_async_small<sizeof(T)>(sc + i,
+                                    ok ? src + j * cm.N + g[0] + (long long)cm.nn[0] * (g[1] + (long long)cm.nn[1] * g[2])
+                                       : src,
+                                    ok);
         }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncthreads();
+      // x: sc[z][y][cx] -> s1[z][y][fx]
+      for (int i = threadIdx.x; i < NZC * LC * LF; i += blockDim.x)
+        {
+          const int fx = i % LF, r = i / LF;
+          const int cc = min(fx / (2 * P), C - 1), t = fx - 2 * P * cc;
+          const T  *in = sc + r * LC + P * cc;
+          T         v  = T(0);
+#pragma unroll
+          for (int b = 0; b <= P; ++b)
+            v += W.w[t][b] * in[b];
+          s1[i] = v;
+        }
+      __syncthreads();
+      // y: s1[z][cy][fx] -> s2[z][fy][fx]
+      for (int i = threadIdx.x; i < NZC * LF * LF; i += blockDim.x)
+        {
+          const int fx = i % LF, fy = (i / LF) % LF, z = i / (LF * LF);
+          const int cc = min(fy / (2 * P), C - 1), t = fy - 2 * P * cc;
+          const T  *in = s1 + (z * LC + P * cc) * LF + fx;
+          T         v  = T(0);
+#pragma unroll
+          for (int b = 0; b <= P; ++b)
+            v += W.w[t][b] * in[b * LF];
+          s2[i] = v;
+        }
+      __syncthreads();
+      // z (3-D): s2[cz][fy][fx] -> fine, added to dst
+      batched_add<8>(NZF * LF * LF, dst, [&](int i, long long &off, T &v) {
+        const int fx = i % LF, fy = (i / LF) % LF, fz = i / (LF * LF);
+        const int g[3] = {f0[0] + fx, f0[1] + fy, DIM == 3 ? f0[2] + fz : 0};
+        // owned: below the next tile's first node, or the mesh's last node
+        bool own = (fx < LF - 1 || g[0] == fm.nn[0] - 1) && (fy < LF - 1 || g[1] == fm.nn[1] - 1);
+        if (DIM == 3)
+          own = own && (fz < LF - 1 || g[2] == fm.nn[2] - 1);
+        own = own && g[0] < fm.nn[0] && g[1] < fm.nn[1] && (DIM < 3 || g[2] < fm.nn[2]);
+        if (!own || is_boundary_node(fm, g[0], g[1], g[2]))
+          return false;
+        if constexpr (DIM == 3)
+          {
+            const int cc = min(fz / (2 * P), C - 1), t = fz - 2 * P * cc;
+            const T  *in = s2 + (P * cc) * LF * LF + fy * LF + fx;
+            v            = T(0);
+#pragma unroll
+            for (int b = 0; b <= P; ++b)
+              v += W.w[t][b] * in[b * LF * LF];
+          }
+        else
+          v = s2[i];
+        off = j * fm.N + g[0] + (long long)fm.nn[0] * (g[1] + (long long)fm.nn[1] * g[2]);
+        return true;
+      });
     }
 
     // Restriction dst_c += P^T src_f, one CTA per tile of C^dim coarse cells
-    // owning coarse nodes [PC t, PC (t+1)) (the last node to the last tile):
-    // the fine block [2P(C t - 1), 2P C (t+1)] per direction (Dirichlet and
-    // outside nodes zero) is reduced direction by direction. A coarse vertex
-    // collects the fine nodes of both neighbouring coarse cells, the shared
-    // fine vertex once.
+    // and time dof (blockIdx.y), owning coarse nodes [PC t, PC (t+1)) (the
+    // last node to the last tile): the fine block [2P(C t - 1), 2P C (t+1)]
+    // per direction (Dirichlet and outside nodes zero) is reduced direction
+    // by direction. A coarse vertex collects the fine nodes of both
+    // neighbouring coarse cells, the shared fine vertex once.
     template <int DIM, int P, int C, typename T>
     __global__ void __launch_bounds__(256)
-    h_restrict_tiled(const MeshView fm, const MeshView cm, int nt, const __grid_constant__ HWeights<T> W,
+    h_restrict_tiled(const MeshView fm, const MeshView cm, const __grid_constant__ HWeights<T> W,
                      const T *__restrict__ src, T *__restrict__ dst)
     {
       constexpr int LR = 2 * P * (C + 1) + 1, LQ = P * C + 1;
@@ -161,7 +186,7 @@ namespace stmg
       T *s1 = sf + NZR * LR * LR;   // [z][y][qx]
       T *s2 = s1 + NZR * LR * LQ;   // [z][qy][qx]
       const int ntx = (cm.n[0] + C - 1) / C, nty = (cm.n[1] + C - 1) / C;
-      const int tile = blockIdx.x;
+      const int tile = blockIdx.x, j = blockIdx.y;
       const int t0 = tile % ntx, t1 = (tile / ntx) % nty, t2 = DIM == 3 ? tile / (ntx * nty) : 0;
       const int q0[3] = {t0 * C * P, t1 * C * P, t2 * C * P};
       const int fo[3] = {2 * P * (t0 * C - 1), 2 * P * (t1 * C - 1), 2 * P * (t2 * C - 1)};
@@ -184,52 +209,48 @@ namespace stmg
           }
         return v;
       };
-      for (int j = 0; j < nt; ++j)
+      for (int i = threadIdx.x; i < NZR * LR * LR; i += blockDim.x)
         {
-          for (int i = threadIdx.x; i < NZR * LR * LR; i += blockDim.x)
-            {
-              const int x = i % LR, y = (i / LR) % LR, z = i / (LR * LR);
-              const int g[3] = {fo[0] + x, fo[1] + y, DIM == 3 ? fo[2] + z : 0};
-              bool      ok   = g[0] >= 0 && g[1] >= 0 && g[0] < fm.nn[0] && g[1] < fm.nn[1];
-              if (DIM == 3)
-                ok = ok && g[2] >= 0 && g[2] < fm.nn[2];
-              ok = ok && !is_boundary_node(fm, g[0], g[1], g[2]);
-              // asynchronous copy (zero fill outside): all loads of the block in flight at once
-              cp_async_small<sizeof(T)>(sf + i,
-                                        ok ? src + j * fm.N + g[0] + (long long)fm.nn[0] * (g[1] + (long long)fm.nn[1] * g[2])
-                                           : src,
-                                        ok);
-            }
-          cp_async_commit();
-          cp_async_wait<0>();
-          __syncthreads();
-          for (int i = threadIdx.x; i < NZR * LR * LQ; i += blockDim.x)
-            {
-              const int qx = i % LQ, r = i / LQ;
-              s1[i]        = reduce1(sf + r * LR, 1, qx);
-            }
-          __syncthreads();
-          for (int i = threadIdx.x; i < NZR * LQ * LQ; i += blockDim.x)
-            {
-              const int qx = i % LQ, qy = (i / LQ) % LQ, z = i / (LQ * LQ);
-              s2[i]        = reduce1(s1 + z * LR * LQ + qx, LQ, qy);
-            }
-          __syncthreads();
-          for (int i = threadIdx.x; i < NZQ * LQ * LQ; i += blockDim.x)
-            {
-              const int qx = i % LQ, qy = (i / LQ) % LQ, qz = i / (LQ * LQ);
-              const int g[3] = {q0[0] + qx, q0[1] + qy, DIM == 3 ? q0[2] + qz : 0};
-              bool own = (qx < LQ - 1 || g[0] == cm.nn[0] - 1) && (qy < LQ - 1 || g[1] == cm.nn[1] - 1);
-              if (DIM == 3)
-                own = own && (qz < LQ - 1 || g[2] == cm.nn[2] - 1);
-              own = own && g[0] < cm.nn[0] && g[1] < cm.nn[1] && (DIM < 3 || g[2] < cm.nn[2]);
-              if (!own || is_boundary_node(cm, g[0], g[1], g[2]))
-                continue;
-              const T v = DIM == 3 ? reduce1(s2 + qy * LQ + qx, LQ * LQ, qz) : s2[i];
-              dst[j * cm.N + g[0] + (long long)cm.nn[0] * (g[1] + (long long)cm.nn[1] * g[2])] += v;
-            }
-          __syncthreads();
+          const int x = i % LR, y = (i / LR) % LR, z = i / (LR * LR);
+          const int g[3] = {fo[0] + x, fo[1] + y, DIM == 3 ? fo[2] + z : 0};
+          bool      ok   = g[0] >= 0 && g[1] >= 0 && g[0] < fm.nn[0] && g[1] < fm.nn[1];
+          if (DIM == 3)
+            ok = ok && g[2] >= 0 && g[2] < fm.nn[2];
+          ok = ok && !is_boundary_node(fm, g[0], g[1], g[2]);
+          // asynchronous copy (zero fill outside): all loads of the block in flight at once
+          cp_async_small<sizeof(T)>(sf + i,
+                                    ok ? src + j * fm.N + g[0] + (long long)fm.nn[0] * (g[1] + (long long)fm.nn[1] * g[2])
+                                       : src,
+                                    ok);
         }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncthreads();
+      for (int i = threadIdx.x; i < NZR * LR * LQ; i += blockDim.x)
+        {
+          const int qx = i % LQ, r = i / LQ;
+          s1[i]        = reduce1(sf + r * LR, 1, qx);
+        }
+      __syncthreads();
+      for (int i = threadIdx.x; i < NZR * LQ * LQ; i += blockDim.x)
+        {
+          const int qx = i % LQ, qy = (i / LQ) % LQ, z = i / (LQ * LQ);
+          s2[i]        = reduce1(s1 + z * LR * LQ + qx, LQ, qy);
+        }
+      __syncthreads();
+      batched_add<4>(NZQ * LQ * LQ, dst, [&](int i, long long &off, T &v) {
+        const int qx = i % LQ, qy = (i / LQ) % LQ, qz = i / (LQ * LQ);
+        const int g[3] = {q0[0] + qx, q0[1] + qy, DIM == 3 ? q0[2] + qz : 0};
+        bool own = (qx < LQ - 1 || g[0] == cm.nn[0] - 1) && (qy < LQ - 1 || g[1] == cm.nn[1] - 1);
+        if (DIM == 3)
+          own = own && (qz < LQ - 1 || g[2] == cm.nn[2] - 1);
+        own = own && g[0] < cm.nn[0] && g[1] < cm.nn[1] && (DIM < 3 || g[2] < cm.nn[2]);
+        if (!own || is_boundary_node(cm, g[0], g[1], g[2]))
+          return false;
+        v   = DIM == 3 ? reduce1(s2 + qy * LQ + qx, LQ * LQ, qz) : s2[i];
+        off = j * cm.N + g[0] + (long long)cm.nn[0] * (g[1] + (long long)cm.nn[1] * g[2]);
+        return true;
+      });
     }
 
     template <int DIM, int P, typename T>
@@ -241,16 +262,17 @@ namespace stmg
       long long     tiles = 1;
       for (int d = 0; d < DIM; ++d)
         tiles *= (c.n[d] + C - 1) / C;
+      const dim3 grid{unsigned(tiles), unsigned(nt), 1u};
       if (prolong)
-        h_prolongate_tiled<DIM, P, C, T><<<unsigned(tiles), 256, 0, s>>>(f, c, nt, W, src, dst);
+        h_prolongate_tiled<DIM, P, C, T><<<grid, 256, 0, s>>>(f, c, W, src, dst);
       else
         {
           constexpr int LR = 2 * P * (C + 1) + 1, LQ = P * C + 1, NZR = DIM == 3 ? LR : 1;
-          const std::size_t smem = sizeof(T) * (std::size_t(NZR) * LR * LR + std::size_t(NZR) * LR * LQ +
-                                                std::size_t(NZR) * LQ * LQ);
+          constexpr std::size_t smem = sizeof(T) * (std::size_t(NZR) * LR * LR + std::size_t(NZR) * LR * LQ +
+                                                    std::size_t(NZR) * LQ * LQ);
           auto kern = h_restrict_tiled<DIM, P, C, T>;
           STMG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-          kern<<<unsigned(tiles), 256, smem, s>>>(f, c, nt, W, src, dst);
+          kern<<<grid, 256, smem, s>>>(f, c, W, src, dst);
         }
       count_launch();
       STMG_CUDA(cudaGetLastError());

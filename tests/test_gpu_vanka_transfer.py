@@ -66,7 +66,10 @@ def test_vanka_matches_oracle(case, mode):
 
 
 H_CASES = [(2, (2, 3), 1), (2, (2, 2), 2), (2, (3, 2), 3), (2, (2, 2), 4), (2, (2, 2), 5), (3, (2, 2, 2), 1), (3, (2, 2, 1), 2),
-           (3, (1, 2, 2), 3)]
+           (3, (1, 2, 2), 3),
+           # several tiles per direction, partial last tiles (FP32 tiles of
+           # 16 / 8 / 4 coarse cells for degree 1 in 2-D / 1 in 3-D / 2 in 3-D)
+           (2, (20, 9), 1), (3, (10, 3, 9), 1), (3, (9, 5, 6), 2), (3, (3, 4, 5), 4)]
 
 
 @pytest.mark.parametrize("case", H_CASES, ids=lambda c: f"d{c[0]}-p{c[2]}")
