@@ -424,6 +424,8 @@ namespace stmg
     if (streamed)
       {
         const std::size_t ntp = nt == 3 ? 4 : nt;
+        if (slotrec)
+          return (std::size_t(1) << dim) * (rec_bytes + 4 * 2 * std::size_t(mesh->nd) * ntp) + 4 * nb * ntp;
         if (mmarec)
           return std::size_t(stages) * colour_cells * rec_bytes + 4 * 3 * nb * ntp +
                  vanka_detail::VR_WARPS * 32 * 16 + 128;
@@ -811,10 +813,20 @@ namespace stmg
       rowrec = streamed && teig.use && nd <= 32 && nreal == nt % 2 && !(e && e[0] == '0');
     }
     {
+      // the small-tile apply where the colour-phase tiles would leave SMs
+      // idle (STMG_VANKA_SLOT=0 / 1 turns it off / on for every row-record
+      // mesh)
+      const char *e = std::getenv("STMG_VANKA_SLOT");
+      int         sh[3];
+      vanka_shape(dim, p, true, sh);
+      const bool few = make_tiling(mesh->v, sh).n_tiles < sm_count();
+      slotrec        = rowrec && (e ? e[0] == '1' : few);
+    }
+    {
       // the tensor-core apply: BF16 storage, 3 or 4 time dofs (one brick word
       // of four FP32 per node)
       const char *e = std::getenv("STMG_VANKA_MMA");
-      mmarec        = rowrec && storage == STMG_BF16 && (nt == 3 || nt == 4) && !(e && e[0] == '0');
+      mmarec = rowrec && !slotrec && storage == STMG_BF16 && (nt == 3 || nt == 4) && !(e && e[0] == '0');
     }
     if (mmarec)
       {
@@ -866,7 +878,17 @@ namespace stmg
         mu_off     = int(pad(nd * nd * elem));
         rec_bytes  = int(pad(mu_off + nd * (compute == STMG_F64 ? 8 : 4)));
       }
-    bool ok  = false;
+    bool ok = false;
+    if (slotrec)
+      {
+        shape[0] = shape[1] = 2;
+        shape[2]            = dim == 3 ? 2 : 1;
+        tiling              = make_tiling(mesh->v, shape);
+        colour_cells        = 1;
+        big                 = false;
+        ok                  = smem_bytes(shape) <= 200 * 1024;
+        slotrec             = ok;
+      }
     for (bool b : {true, false})
       {
         if (!streamed || ok)

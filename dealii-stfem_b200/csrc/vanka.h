@@ -104,6 +104,10 @@ namespace stmg
     // applied by the tensor-core kernel (3 or 4 time dofs, nd <= 32); teig_pf
     // is teig with complex pairs first (the kernel's lane layout)
     bool                  mmarec = false;
+    // slotrec: row records on tiles of 2^dim cells applied by the small-tile
+    // kernel (all cells of a tile at once, per-cell output slots): meshes
+    // whose colour-phase tiles would occupy fewer CTAs than there are SMs
+    bool                  slotrec = false;
     // record stages of the row-record and tensor-core applies (3..5): as
     // many colour phases in flight as two CTAs per SM leave room for
     int                   stages = 3;

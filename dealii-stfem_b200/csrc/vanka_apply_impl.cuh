@@ -869,6 +869,63 @@ namespace stmg
         v[i] = o[i];
     }
 
+    // A tile's output brick (accumulated in the eigenbasis) back through S
+    // and out, as in the streamed apply: tile-interior nodes to dst through
+    // the output mode, weighted by 1/valence; shell nodes to the tile's face
+    // slots, or the constrained write when one tile covers the mesh. nw
+    // warps walk brick rows, 32 / E0 rows per warp step.
+    template <int DIM, int P, int NT, typename S>
+    __device__ __forceinline__ void
+    row_tile_output(const MeshView &m, const Tiling &tl, const TimeEig &te, const TileGeo &tg, int tile,
+                    const float *bout, float *__restrict__ dst, float *__restrict__ shell, const OutMode<float> &om,
+                    int nw)
+    {
+      using TV           = TimeVec<NT>;
+      constexpr int NTP  = TV::NTP;
+      constexpr int RPW  = 32 / S::E0;
+      const int     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const int     lrow = lane / S::E0, lx = lane - lrow * S::E0;
+      const int     gx   = tg.c0[0] * P + lx;
+      const int     vx   = (gx % P == 0) ? 2 : 1;
+      const bool    inx  = lx > 0 && lx < tg.e[0] - 1;
+      for (int rb = warp * RPW; rb < S::E1 * S::E2; rb += nw * RPW)
+        {
+          const int row = rb + lrow;
+          if (lrow >= RPW || row >= S::E1 * S::E2 || lx >= tg.e[0])
+            continue;
+          const int bz = row / S::E1, by = row - bz * S::E1;
+          if (by >= tg.e[1] || bz >= tg.e[2])
+            continue;
+          bool inte = inx && by > 0 && by < tg.e[1] - 1;
+          if (DIM == 3)
+            inte = inte && bz > 0 && bz < tg.e[2] - 1;
+          const int gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
+          int       v  = vx * ((gy % P == 0) ? 2 : 1);
+          if (DIM == 3)
+            v *= (gz % P == 0) ? 2 : 1;
+          const float w = v == 1 ? 1.0f : (v == 2 ? 0.5f : (v == 4 ? 0.25f : 0.125f));
+          float       o[NT];
+          TV::load(bout + ((bz * S::E1 + by) * S::E0 + lx) * NTP, o);
+          time_map<NT>(te.S, o);
+          long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+          if (inte)
+#pragma unroll
+            for (int jt = 0; jt < NT; ++jt, gi += m.N)
+              om.write(dst, gi, o[jt] * w);
+          else if (tl.n_tiles == 1)
+#pragma unroll
+            for (int jt = 0; jt < NT; ++jt, gi += m.N)
+              om.write_constrained(dst, gi);
+          else
+            {
+              float *sj = shell + (long long)tile * NT * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz);
+#pragma unroll
+              for (int jt = 0; jt < NT; ++jt, sj += tl.tile_stride)
+                *sj = o[jt];
+            }
+        }
+    }
+
     // Row-record apply: as the streamed apply (colour phases, records in
     // (tile, colour, cell) order, one warp per cell, one output brick per
     // tile), but
@@ -1114,47 +1171,7 @@ namespace stmg
           if (col == NC - 1)
             {
               __syncthreads();
-              // the tile's output (back from the eigenbasis: o <- S o), as in
-              // the streamed apply
-              const int  gx  = tg.c0[0] * P + lx;
-              const int  vx  = (gx % P == 0) ? 2 : 1;
-              const bool inx = lx > 0 && lx < tg.e[0] - 1;
-              for (int rb = warp * RPW; rb < S::E1 * S::E2; rb += NW * RPW)
-                {
-                  const int row = rb + lrow;
-                  if (lrow >= RPW || row >= S::E1 * S::E2 || lx >= tg.e[0])
-                    continue;
-                  const int bz = row / S::E1, by = row - bz * S::E1;
-                  if (by >= tg.e[1] || bz >= tg.e[2])
-                    continue;
-                  bool inte = inx && by > 0 && by < tg.e[1] - 1;
-                  if (DIM == 3)
-                    inte = inte && bz > 0 && bz < tg.e[2] - 1;
-                  const int gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
-                  int       v  = vx * ((gy % P == 0) ? 2 : 1);
-                  if (DIM == 3)
-                    v *= (gz % P == 0) ? 2 : 1;
-                  const float w = v == 1 ? 1.0f : (v == 2 ? 0.5f : (v == 4 ? 0.25f : 0.125f));
-                  float       o[NT];
-                  TV::load(bout + ((bz * S::E1 + by) * S::E0 + lx) * NTP, o);
-                  time_map<NT>(te.S, o);
-                  long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
-                  if (inte)
-#pragma unroll
-                    for (int jt = 0; jt < NT; ++jt, gi += m.N)
-                      om.write(dst, gi, o[jt] * w);
-                  else if (tl.n_tiles == 1)
-#pragma unroll
-                    for (int jt = 0; jt < NT; ++jt, gi += m.N)
-                      om.write_constrained(dst, gi);
-                  else
-                    {
-                      float *sj = shell + (long long)tile * NT * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz);
-#pragma unroll
-                      for (int jt = 0; jt < NT; ++jt, sj += tl.tile_stride)
-                        *sj = o[jt];
-                    }
-                }
+              row_tile_output<DIM, P, NT, S>(m, tl, te, tg, tile, bout, dst, shell, om, NW);
               __syncthreads();
               for (int idx = threadIdx.x; idx < S::NB * NTP; idx += blockDim.x)
                 bout[idx] = 0.0f;
@@ -1174,6 +1191,214 @@ namespace stmg
           __syncthreads();
         }
       cp_async_wait<0>();
+    }
+
+    // Small-tile apply over the row records, for meshes whose colour-phase
+    // tiles leave most SMs idle: tiles of 2^dim cells, one cell per colour,
+    // whose 2^dim records arrive together, and one warp per cell for all of
+    // them at once. Each cell's V^T w goes to a slot of its own; each brick
+    // node then sums the slots of its cells in colour order, the order in
+    // which the colour phases of vanka_row_kernel add them. A tile costs one
+    // cell's latency instead of 2^dim phases of it. Records, input brick, G
+    // and S maps, output modes and face slots as in vanka_row_kernel.
+    template <int DIM, int P, typename TS, int NT>
+    __global__ void __launch_bounds__(32 << DIM)
+    vanka_slot_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeEig te,
+                      const unsigned char *__restrict__ rec, int rec_bytes, int mu_off, const float *__restrict__ src,
+                      float *__restrict__ dst, float *__restrict__ shell, const OutMode<float> om)
+    {
+      using S            = TileShape<DIM, P, 2, 2, 2>;
+      using TV           = TimeVec<NT>;
+      using RW           = RowWord<TS>;
+      using W            = typename RW::W;
+      constexpr int ND   = S::ND;
+      constexpr int NTP  = TV::NTP;
+      constexpr int NA   = (NTP + 1) / 2;
+      constexpr int NR   = NT % 2;
+      constexpr int NC   = 1 << DIM;
+      constexpr int P1   = P + 1;
+      constexpr int RS   = vk_row_stride<TS>(ND);
+      constexpr int RWD  = RS / RW::PER;
+      constexpr int RPW  = 32 / S::E0;
+      constexpr int ROWS = NT * S::E1 * S::E2;
+      constexpr bool MU_IN_ROW = sizeof(TS) == 4;
+      static_assert(ND <= 32, "small-tile apply: at most 32 dofs per cell");
+      static_assert(S::E0 <= 32, "brick rows wider than a warp");
+      extern __shared__ __align__(16) unsigned char vk_smem[];
+      // records [NC][rec_bytes] | brick [NB][NTP] (input, then output) |
+      // slots [NC][ND][NTP] | mode values [NC][ND][NTP]
+      float    *brick = reinterpret_cast<float *>(vk_smem + NC * rec_bytes);
+      float    *slots = brick + S::NB * NTP;
+      float    *wbuf  = slots + NC * ND * NTP;
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const int lrow = lane / S::E0, lx = lane - lrow * S::E0;
+      const int cx = warp & 1, cy = (warp >> 1) & 1, cz = (warp >> 2) & 1; // this warp's cell (= colour)
+      const int r16 = NC * rec_bytes / 16;
+
+      for (int tile = blockIdx.x; tile < tl.n_tiles; tile += gridDim.x)
+        {
+          const TileGeo tg = tile_geo<DIM, P>(m, tl, tile);
+          // the tile's records (slot c holds the cell of colour c) and its
+          // input brick, one group of asynchronous copies
+          const unsigned char *g = rec + (long long)tile * NC * rec_bytes;
+          for (int q = threadIdx.x; q < r16; q += blockDim.x)
+            cp_async16(vk_smem + 16 * q, g + 16 * q);
+          {
+            const int  gx  = tg.c0[0] * P + lx;
+            const bool okx = lx < tg.e[0] && gx > 0 && gx < m.nn[0] - 1;
+            for (int rb = warp * RPW; rb < ROWS; rb += NC * RPW)
+              {
+                const int row = rb + lrow;
+                if (lrow >= RPW || row >= ROWS)
+                  continue;
+                const int i = row / (S::E1 * S::E2), rem = row - i * (S::E1 * S::E2);
+                const int bz = rem / S::E1, by = rem - bz * S::E1;
+                const int gy = tg.c0[1] * P + by, gz = tg.c0[2] * P + bz;
+                bool      ok = okx && by < tg.e[1] && bz < tg.e[2] && gy > 0 && gy < m.nn[1] - 1;
+                if (DIM == 3)
+                  ok = ok && gz > 0 && gz < m.nn[2] - 1;
+                const float *gp = ok ? src + i * m.N + gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz) : src;
+                cp_async_small<4>(brick + ((bz * S::E1 + by) * S::E0 + lx) * NTP + i, gp, ok);
+              }
+          }
+          cp_async_commit();
+          cp_async_wait<0>();
+          __syncthreads();
+          // the input in the eigenbasis: x <- G x per node
+          for (int nd = threadIdx.x; nd < S::NB; nd += blockDim.x)
+            {
+              float v[NT];
+              TV::load(brick + nd * NTP, v);
+              time_map<NT>(te.G, v);
+              TV::store(brick + nd * NTP, v);
+            }
+          __syncthreads();
+          const bool live = cx < tg.tc[0] && cy < tg.tc[1] && (DIM < 3 || cz < tg.tc[2]);
+          if (live)
+            {
+              const unsigned char *r     = vk_smem + warp * rec_bytes;
+              const TS            *V     = reinterpret_cast<const TS *>(r);
+              const int            bbase = cx * P + S::E0 * (cy * P + S::E1 * (cz * P));
+              float               *wb    = wbuf + warp * ND * NTP;
+              // pass 1 (lane = mode): y = V x, then the mode's time solve
+              {
+                const int mm  = lane < ND ? lane : ND - 1;
+                const W  *row = reinterpret_cast<const W *>(V + mm * RS);
+                W         vw[RWD];
+#pragma unroll
+                for (int q = 0; q < RWD; ++q)
+                  vw[q] = row[q];
+                float2 ya[NA], yb[NA];
+#pragma unroll
+                for (int q = 0; q < NA; ++q)
+                  ya[q] = yb[q] = make_float2(0.0f, 0.0f);
+#pragma unroll
+                for (int a = 0; a < ND; ++a)
+                  {
+                    const float  v = RW::get(vw[a / RW::PER], a % RW::PER);
+                    const float *x = brick + (bbase + S::offset(a)) * NTP;
+                    if (a & 1)
+                      acc_time<NTP>(yb, v, x);
+                    else
+                      acc_time<NTP>(ya, v, x);
+                  }
+                float mu;
+                if constexpr (MU_IN_ROW)
+                  mu = RW::get(vw[ND / RW::PER], ND % RW::PER);
+                else
+                  mu = reinterpret_cast<const float *>(r + mu_off)[mm];
+                float y[NT];
+#pragma unroll
+                for (int i = 0; i < NT; ++i)
+                  y[i] = (i & 1) ? ya[i / 2].y + yb[i / 2].y : ya[i / 2].x + yb[i / 2].x;
+                mode_scale<NT, NR>(te, mu, y);
+                if (lane < ND)
+                  TV::store(wb + lane * NTP, y);
+              }
+              __syncwarp();
+              // pass 2 (lane = dof): V^T w into this cell's slot
+              {
+                const int a = lane < ND ? lane : ND - 1;
+                float2    oa[NA], ob[NA];
+#pragma unroll
+                for (int q = 0; q < NA; ++q)
+                  oa[q] = ob[q] = make_float2(0.0f, 0.0f);
+#pragma unroll 9
+                for (int mm = 0; mm < ND; ++mm)
+                  {
+                    const float v = load_s(V + mm * RS + a);
+                    if (mm & 1)
+                      acc_time<NTP>(ob, v, wb + mm * NTP);
+                    else
+                      acc_time<NTP>(oa, v, wb + mm * NTP);
+                  }
+                if (lane < ND)
+                  {
+                    float o[NT];
+#pragma unroll
+                    for (int i = 0; i < NT; ++i)
+                      o[i] = (i & 1) ? oa[i / 2].y + ob[i / 2].y : oa[i / 2].x + ob[i / 2].x;
+                    TV::store(slots + (warp * ND + lane) * NTP, o);
+                  }
+              }
+            }
+          __syncthreads();
+          // each brick node: the slots of its live cells in colour order
+          // (into the brick buffer, whose input nobody reads any more)
+          for (int nd = threadIdx.x; nd < S::NB; nd += blockDim.x)
+            {
+              const int bx = nd % S::E0, by = (nd / S::E0) % S::E1, bz = nd / (S::E0 * S::E1);
+              float     acc[NT];
+#pragma unroll
+              for (int i = 0; i < NT; ++i)
+                acc[i] = 0.0f;
+#pragma unroll
+              for (int c = 0; c < NC; ++c)
+                {
+                  const int ux = c & 1, uy = (c >> 1) & 1, uz = (c >> 2) & 1;
+                  const int ax = bx - ux * P, ay = by - uy * P, az = bz - uz * P;
+                  bool      in = ax >= 0 && ax <= P && ay >= 0 && ay <= P && ux < tg.tc[0] && uy < tg.tc[1];
+                  if (DIM == 3)
+                    in = in && az >= 0 && az <= P && uz < tg.tc[2];
+                  if (in)
+                    {
+                      const int a = ax + P1 * (ay + (DIM == 3 ? P1 * az : 0));
+                      float     o[NT];
+                      TV::load(slots + (c * ND + a) * NTP, o);
+#pragma unroll
+                      for (int i = 0; i < NT; ++i)
+                        acc[i] += o[i];
+                    }
+                }
+              TV::store(brick + nd * NTP, acc);
+            }
+          __syncthreads();
+          row_tile_output<DIM, P, NT, S>(m, tl, te, tg, tile, brick, dst, shell, om, NC);
+          __syncthreads();
+        }
+      cp_async_wait<0>();
+    }
+
+    template <int DIM, int P, typename TS, int NT>
+    void
+    launch_slot(const Vanka &vk, const float *src, float *dst, const OutMode<float> &om, cudaStream_t s)
+    {
+      if constexpr (Tens<P + 1, DIM>::ND <= 32)
+        {
+          const MeshView   &m    = vk.mesh->v;
+          const Tiling     &tl   = vk.tiling;
+          const std::size_t smem = vk.smem_bytes(vk.shape);
+          auto              kern = vanka_slot_kernel<DIM, P, TS, NT>;
+          const unsigned    grid = persistent_grid(reinterpret_cast<const void *>(kern), 32 << DIM, smem, tl.n_tiles);
+          kern<<<grid, 32 << DIM, smem, s>>>(m, tl, vk.teig, vk.V.ptr, vk.rec_bytes, vk.mu_off, src, dst,
+                                             reinterpret_cast<float *>(vk.shell.ptr), om);
+          count_launch();
+          STMG_CUDA(cudaGetLastError());
+          if (tl.n_tiles > 1)
+            launch_plane_fixup<DIM, float, true>(m, tl, vk.nt, reinterpret_cast<float *>(vk.shell.ptr), dst, om, s);
+        }
+      else
+        throw Error(STMG_ERR_UNSUPPORTED, "vanka: row records need at most 32 dofs per cell");
     }
 
     // ---------------------------------------------- tensor-core apply
@@ -1704,6 +1929,8 @@ namespace stmg
               launch_mma<DIM, P, NT, false>(vk, src, dst, om, s);
             return;
           }
+      if (vk.slotrec)
+        return launch_slot<DIM, P, TS, NT>(vk, src, dst, om, s);
       if (vk.rowrec)
         {
           if (vk.big)

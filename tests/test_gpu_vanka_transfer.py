@@ -150,6 +150,7 @@ def test_vanka_row_records_match_streamed_and_oracle(monkeypatch, case, storage)
     om, gm, A, B, src = _setup(case)
     ref = om.vanka_apply(A, B, src)
     st = stmg.F32 if storage == "f32" else stmg.BF16
+    monkeypatch.setenv("STMG_VANKA_SLOT", "0")  # the colour-phase kernels on these small meshes
     monkeypatch.setenv("STMG_VANKA_ROWREC", "1")
     vr = stmg.Vanka(gm, A, B, compute=stmg.F32, storage=st)
     monkeypatch.setenv("STMG_VANKA_ROWREC", "0")
@@ -185,6 +186,7 @@ def test_vanka_tensor_core_matches_row_kernel(monkeypatch, case):
     import stmg
     om, gm, A, B, src = _setup(case)
     ref = om.vanka_apply(A, B, src)
+    monkeypatch.setenv("STMG_VANKA_SLOT", "0")
     monkeypatch.setenv("STMG_VANKA_MMA", "1")
     vm = stmg.Vanka(gm, A, B, compute=stmg.F32, storage=stmg.BF16)
     monkeypatch.setenv("STMG_VANKA_MMA", "0")
@@ -199,3 +201,50 @@ def test_vanka_tensor_core_matches_row_kernel(monkeypatch, case):
     assert rel2(got, row) <= 1e-4, rel2(got, row)
     assert rel2(got, ref) <= 3e-2, rel2(got, ref)
 
+
+
+SLOT_CASES = ROW_CASES + [
+    (3, (16, 16, 16), 2, 0.0, True, (orc.DG, 3, 1, orc.HEAT)),
+    (3, (7, 5, 9), 2, 0.15, True, (orc.DG, 2, 1, orc.HEAT)),
+    (2, (15, 22), 4, 0.1, True, (orc.CGP, 2, 1, orc.HEAT)),
+]
+
+
+@pytest.mark.parametrize("case", SLOT_CASES, ids=lambda c: f"d{c[0]}-p{c[2]}-r{c[5][1]}-n{'x'.join(map(str, c[1]))}")
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+def test_vanka_small_tiles_match_row_kernel_and_oracle(monkeypatch, case, storage):
+    """The small-tile apply (tiles of 2^dim cells, all cells of a tile at
+    once, per-cell output slots summed in colour order; STMG_VANKA_SLOT=1)
+    against the colour-phase row kernel over row records of the same
+    storage (STMG_VANKA_SLOT=0, tensor-core apply off): the same cell
+    arithmetic on other tile boundaries, so agreement to FP32 rounding of
+    the node sums (2e-6); and against the oracle's Gauss-Jordan inverses.
+    Both the plain apply and the relaxation update x += omega V (b - A x)."""
+    import stmg
+    om, gm, A, B, src = _setup(case)
+    ref = om.vanka_apply(A, B, src)
+    st = stmg.F32 if storage == "f32" else stmg.BF16
+    monkeypatch.setenv("STMG_VANKA_MMA", "0")
+    monkeypatch.setenv("STMG_VANKA_SLOT", "1")
+    vt = stmg.Vanka(gm, A, B, compute=stmg.F32, storage=st)
+    monkeypatch.setenv("STMG_VANKA_SLOT", "0")
+    vr = stmg.Vanka(gm, A, B, compute=stmg.F32, storage=st)
+    s = torch.tensor(src, dtype=torch.float32, device="cuda")
+    dt, dr = torch.full_like(s, 3.0), torch.full_like(s, -1.0)
+    for _ in range(2):
+        vt.vmult(dt, s)
+        vr.vmult(dr, s)
+    torch.cuda.synchronize()
+    got, row = dt.double().cpu().numpy(), dr.double().cpu().numpy()
+    assert rel2(got, ref) <= (2e-4 if storage == "f32" else 3e-2), rel2(got, ref)
+    assert rel2(got, row) <= 2e-6, rel2(got, row)
+    # relaxation step through both kernels' output modes
+    op = stmg.Operator(gm, A, B, dtype=stmg.F32)
+    b = torch.tensor(meshes.random_block_vector(A.shape[0], om.n_nodes, meshes.boundary_mask(case[0], case[1], case[2]),
+                                                seed=11), dtype=torch.float32, device="cuda")
+    xt, xr = s.clone(), s.clone()
+    tmp = torch.empty_like(s)
+    vt.step(op, 0.7, xt, b, tmp)
+    vr.step(op, 0.7, xr, b, tmp)
+    torch.cuda.synchronize()
+    assert rel2(xt.double().cpu().numpy(), xr.double().cpu().numpy()) <= 2e-6
