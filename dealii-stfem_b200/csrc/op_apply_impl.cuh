@@ -23,6 +23,7 @@ namespace stmg
     OutMode<T>   om;
     bool         big;
     cudaStream_t s;
+    bool         tiny = false; // 3-D degree 2: tiles of 2x2x2 cells, phase B by planes (small meshes)
   };
 
   // shared memory of the operator kernel for a tile shape: two input bricks
@@ -533,7 +534,7 @@ namespace stmg
     //     tile's face slots (or constrained writes when one tile covers the
     //     mesh).
     // NTPC: 1 or 2 time values per node, or 4 for multiples of four.
-    template <int DIM, int P, typename T, int MODE, int TX, int TY, int TZ, int NTPC>
+    template <int DIM, int P, typename T, int MODE, int TX, int TY, int TZ, int NTPC, bool PL = false>
     __global__ void __launch_bounds__(256, (MODE == 1 || (sizeof(T) == 4 && MODE == 2)) ? 2 : 1)
     st_apply_kernel(const MeshView m, const Tiling tl, const __grid_constant__ TimeMats<T> tm,
                     const __grid_constant__ Cart1D<T> c1, const __grid_constant__ QTab<T> qt,
@@ -543,8 +544,10 @@ namespace stmg
       constexpr int ND = S::ND;
       constexpr int P1 = P + 1;
       constexpr int NW = 8; // warps per CTA
-      // 3-D degree 3: phase B by planes (see planes_apply)
-      constexpr bool PLANES = DIM == 3 && P == 3;
+      // 3-D degree 3, and degree 2 where PL asks for it (the small tiles of
+      // small meshes, whose per-thread cell chains would be the critical
+      // path): phase B by planes (see planes_apply)
+      constexpr bool PLANES = DIM == 3 && (P == 3 || PL);
       extern __shared__ __align__(16) unsigned char smem_raw[];
       const int nti = tm.nt_in, nto = tm.nt_out;
       const int ntp = NTPC == 4 ? (nti + 3) / 4 * 4 : NTPC;
@@ -615,7 +618,9 @@ namespace stmg
                   const int w  = w0 + grp;
                   int       lc = w / nto, j = w - lc * nto;
                   int       lx = lc % TX, ly = (lc / TX) % TY, lz = lc / (TX * TY);
-                  const bool item = w < nto * S::TC && lx < tc[0] && ly < tc[1] && lz < tc[2];
+                  // (lanes past the last full group, for P1 not dividing 32,
+                  // join the shuffles but hold no item)
+                  const bool item = grp < IPW && w < nto * S::TC && lx < tc[0] && ly < tc[1] && lz < tc[2];
                   if (!item)
                     lc = j = lx = ly = lz = 0;
                   const int       cx = c0[0] + lx, cy = c0[1] + ly, cz = c0[2] + lz;
@@ -864,9 +869,15 @@ namespace stmg
   void
   op_launch_variant(const OpLaunch<T> &L)
   {
-    using Sh = op_detail::OpShape<DIM, P, T, BIG>;
+    using Sh  = op_detail::OpShape<DIM, P, T, BIG>;
     auto kern = op_detail::st_apply_kernel<DIM, P, T, MODE, Sh::TX, Sh::TY, Sh::TZ, NTPC>;
-    const int shape[3] = {Sh::TX, Sh::TY, Sh::TZ};
+    int  shape[3] = {Sh::TX, Sh::TY, Sh::TZ};
+    if constexpr (DIM == 3 && P == 2)
+      if (L.tiny)
+        {
+          kern  = op_detail::st_apply_kernel<DIM, P, T, MODE, 2, 2, 2, NTPC, true>;
+          shape[0] = shape[1] = shape[2] = 2;
+        }
     const std::size_t smem = op_smem_bytes(DIM, P, shape, L.tm.nt_in, L.tm.nt_out, sizeof(T));
     const unsigned grid = persistent_grid(reinterpret_cast<const void *>(kern), 256, smem, L.tl.n_tiles);
     kern<<<grid, 256, smem, L.s>>>(L.m, L.tl, L.tm, L.c1, L.qt, L.src, L.dst, L.shell, L.om);

@@ -13,6 +13,8 @@
 #include <mutex>
 #include <string>
 
+#include <cstdlib>
+
 #include "op_apply_impl.cuh"
 #include "st_operator.h"
 
@@ -25,7 +27,8 @@ namespace stmg
     launch(const StOperator &op, bool transpose, const T *src, T *dst, T *shell, const OutMode<T> &om, cudaStream_t s)
     {
       OpLaunch<T> L{op.mesh->v, transpose ? op.tilingT : op.tiling, transpose ? op.tmT<T>() : op.tm<T>(),
-                    op.cart<T>(), op.qtab<T>(), src, dst, shell, om, transpose ? op.bigT : op.big, s};
+                    op.cart<T>(), op.qtab<T>(), src, dst, shell, om, transpose ? op.bigT : op.big, s,
+                    transpose ? op.tinyT : op.tiny};
       const int dim = op.mesh->v.dim, p = op.mesh->v.p;
 #define STMG_CASE(D, PP)                                                                                 \
   if (dim == D && p == PP)                                                                               \
@@ -172,6 +175,26 @@ namespace stmg
     qtab32 = make_qtab<float>(mesh->v.p);
     tiling  = choose_tiling(nt_in, nt_out, big, shp);
     tilingT = choose_tiling(nt_out, nt_in, bigT, shpT);
+    {
+      // 3-D degree 2 on meshes of at most one 2x2x2-cell tile per SM (a
+      // tile of the regular shapes is a long serial chain there): tiles of
+      // 2x2x2 cells, phase B by planes (STMG_OP_TINY=0 / 1 turns it off / on
+      // for every 3-D degree-2 mesh)
+      const char *e   = std::getenv("STMG_OP_TINY");
+      const bool  can = mesh->v.dim == 3 && mesh->v.p == 2;
+      const int   t2[3] = {2, 2, 2};
+      const bool  few   = can && make_tiling(mesh->v, t2).n_tiles <= sm_count();
+      auto        pick  = [&](Tiling &t, int *sh, bool &ti) {
+        ti = can && (e ? e[0] == '1' : few);
+        if (ti)
+          {
+            sh[0] = sh[1] = sh[2] = 2;
+            t                     = make_tiling(mesh->v, sh);
+          }
+      };
+      pick(tiling, shp, tiny);
+      pick(tilingT, shpT, tinyT);
+    }
     const std::size_t elem = dtype == STMG_F64 ? 8 : 4;
     const std::size_t n1   = std::size_t(tiling.n_tiles) * nt_out * tiling.tile_stride;
     const std::size_t n2   = std::size_t(tilingT.n_tiles) * nt_in * tilingT.tile_stride;

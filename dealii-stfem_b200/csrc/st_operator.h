@@ -23,6 +23,7 @@ namespace stmg
     std::vector<double> A, B;
     Tiling              tiling, tilingT;
     bool                big = true, bigT = true; // compile-time tile shape in use
+    bool                tiny = false, tinyT = false; // 2x2x2-cell tiles (3-D degree 2, small meshes)
     int                 shp[3] = {1, 1, 1}, shpT[3] = {1, 1, 1};
 
     template <typename T>

@@ -170,3 +170,54 @@ def test_relax_step_matches_composition(prec):
     tol = 1e-12 if prec == "f64" else 1e-5
     assert torch.linalg.norm(x1 - ref) <= tol * torch.linalg.norm(ref)
     assert torch.linalg.norm(tmp - r) <= tol * torch.linalg.norm(r)
+
+
+TINY_CASES = [c for c in CASES if c[0] == 3 and c[2] == 2] + [
+    (3, (13, 9, 7), 2, 0.1, 1, (orc.DG, 3, 1)),
+    (3, (12, 8, 6), 2, 0.0, 2, (orc.DG, 3, 1)),
+    (3, (8, 8, 8), 2, 0.0, 1, (orc.DG, 2, 1)),
+    (3, (7, 4, 5), 2, 0.0, 0, (orc.CGP, 2, 1)),
+]
+
+
+@pytest.mark.parametrize("case", TINY_CASES, ids=lambda c: f"{'x'.join(map(str, c[1]))}-dist{c[3]}-c{c[4]}-r{c[5][1]}")
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_operator_small_tiles_match_regular_tiles_and_oracle(monkeypatch, case, prec):
+    """3-D degree 2 on tiles of 2x2x2 cells with phase B by planes (three
+    lanes per (cell, time dof), the z sweeps by shuffles; STMG_OP_TINY=1)
+    against the regular tiles with the per-thread phase B (STMG_OP_TINY=0)
+    and the oracle, for vmult, Tvmult and the relaxation update: the same
+    sums in another order and over other tile faces, so FP64 1e-13 / FP32
+    2e-6 between the two."""
+    import stmg
+    om, gm, A, B, rK, rM = build(case)
+    dim, n, p = case[0], case[1], case[2]
+    nt = A.shape[0]
+    mask = meshes.boundary_mask(dim, n, p)
+    src = meshes.random_block_vector(nt, om.n_nodes, mask)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    tol = 1e-12 if prec == "f64" else 2e-5
+    close = 1e-13 if prec == "f64" else 2e-6
+    dty = stmg.F64 if prec == "f64" else stmg.F32
+    monkeypatch.setenv("STMG_OP_TINY", "1")
+    opt = stmg.Operator(gm, A, B, dtype=dty)
+    monkeypatch.setenv("STMG_OP_TINY", "0")
+    opr = stmg.Operator(gm, A, B, dtype=dty)
+    s = torch.tensor(src, dtype=dt, device="cuda")
+    for transpose in (False, True):
+        dp, dq = torch.full_like(s, 7.0), torch.full_like(s, -7.0)
+        (opt.Tvmult if transpose else opt.vmult)(dp, s)
+        (opr.Tvmult if transpose else opr.vmult)(dq, s)
+        ref = om.st_apply(A, B, src, transpose=transpose)
+        got = dp.double().cpu().numpy()
+        assert rel_err(got, ref) < tol
+        assert rel_err(got, dq.double().cpu().numpy()) < close
+    # the residual output mode through a relaxation step (the same FP32 Vanka)
+    if prec == "f32":
+        vk = stmg.Vanka(gm, A, B, compute=stmg.F32, storage=stmg.F32)
+        b = torch.tensor(meshes.random_block_vector(nt, om.n_nodes, mask, seed=5), dtype=dt, device="cuda")
+        xt, xr, tmp = s.clone(), s.clone(), torch.empty_like(s)
+        vk.step(opt, 0.8, xt, b, tmp)
+        vk.step(opr, 0.8, xr, b, tmp)
+        torch.cuda.synchronize()
+        assert rel_err(xt.double().cpu().numpy(), xr.double().cpu().numpy()) < 1e-5
