@@ -173,7 +173,11 @@ namespace stmg
     // last node to the last tile): the fine block [2P(C t - 1), 2P C (t+1)]
     // per direction (Dirichlet and outside nodes zero) is reduced direction
     // by direction. A coarse vertex collects the fine nodes of both
-    // neighbouring coarse cells, the shared fine vertex once.
+    // neighbouring coarse cells, the shared fine vertex once. Every pass runs
+    // by rows: the fine block's rows over the warps with x over the lanes,
+    // the coarse passes GQ rows per warp with the coarse x index over the
+    // lanes (a lane's x and its weights fixed), so the index arithmetic is
+    // per row, not per entry.
     template <int DIM, int P, int C, typename T>
     __global__ void __launch_bounds__(256)
     h_restrict_tiled(const MeshView fm, const MeshView cm, const __grid_constant__ HWeights<T> W,
@@ -181,6 +185,9 @@ namespace stmg
     {
       constexpr int LR = 2 * P * (C + 1) + 1, LQ = P * C + 1;
       constexpr int NZR = DIM == 3 ? LR : 1, NZQ = DIM == 3 ? LQ : 1;
+      constexpr int NW = 8;        // warps (the launch has 256 threads)
+      constexpr int GQ = 32 / LQ;  // coarse rows per warp step
+      static_assert(LQ <= 32, "coarse tile rows wider than a warp");
       extern __shared__ __align__(16) unsigned char hr_smem[];
       T *sf = reinterpret_cast<T *>(hr_smem);
       T *s1 = sf + NZR * LR * LR;   // [z][y][qx]
@@ -190,6 +197,9 @@ namespace stmg
       const int t0 = tile % ntx, t1 = (tile / ntx) % nty, t2 = DIM == 3 ? tile / (ntx * nty) : 0;
       const int q0[3] = {t0 * C * P, t1 * C * P, t2 * C * P};
       const int fo[3] = {2 * P * (t0 * C - 1), 2 * P * (t1 * C - 1), 2 * P * (t2 * C - 1)};
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const int lsub = lane / LQ, lq = lane - lsub * LQ; // lane -> (row in the step, coarse x)
+      const bool lact = lsub < GQ;
       // one direction of P^T: out[q] from in[f], stride s between fine entries
       auto reduce1 = [&](const T *in, int stride, int qx) {
         const int cl = qx / P, k = qx - P * cl; // coarse cell (local) and index in it
@@ -209,48 +219,79 @@ namespace stmg
           }
         return v;
       };
-      for (int i = threadIdx.x; i < NZR * LR * LR; i += blockDim.x)
+      // the fine block: rows (z, y) over the warps, x over the lanes
+      // (asynchronous copies, zero fill outside the interior)
+      for (int r = warp; r < NZR * LR; r += NW)
         {
-          const int x = i % LR, y = (i / LR) % LR, z = i / (LR * LR);
-          const int g[3] = {fo[0] + x, fo[1] + y, DIM == 3 ? fo[2] + z : 0};
-          bool      ok   = g[0] >= 0 && g[1] >= 0 && g[0] < fm.nn[0] && g[1] < fm.nn[1];
-          if (DIM == 3)
-            ok = ok && g[2] >= 0 && g[2] < fm.nn[2];
-          ok = ok && !is_boundary_node(fm, g[0], g[1], g[2]);
-          // asynchronous copy (zero fill outside): all loads of the block in flight at once
-          cp_async_small<sizeof(T)>(sf + i,
-                                    ok ? src + j * fm.N + g[0] + (long long)fm.nn[0] * (g[1] + (long long)fm.nn[1] * g[2])
-                                       : src,
-                                    ok);
+          const int       z = r / LR, y = r - z * LR;
+          const int       gy = fo[1] + y, gz = DIM == 3 ? fo[2] + z : 0;
+          const bool      rin = gy > 0 && gy < fm.nn[1] - 1 && (DIM < 3 || (gz > 0 && gz < fm.nn[2] - 1));
+          const long long roff = j * fm.N + (long long)fm.nn[0] * (gy + (long long)fm.nn[1] * gz);
+#pragma unroll
+          for (int x = lane; x < LR; x += 32)
+            {
+              const int  gx = fo[0] + x;
+              const bool ok = rin && gx > 0 && gx < fm.nn[0] - 1;
+              cp_async_small<sizeof(T)>(sf + r * LR + x, ok ? src + (roff + gx) : src, ok);
+            }
         }
       cp_async_commit();
       cp_async_wait<0>();
       __syncthreads();
-      for (int i = threadIdx.x; i < NZR * LR * LQ; i += blockDim.x)
+      // x: sf[z][y][fx] -> s1[z][y][qx]
+      for (int r0 = warp * GQ; r0 < NZR * LR; r0 += NW * GQ)
         {
-          const int qx = i % LQ, r = i / LQ;
-          s1[i]        = reduce1(sf + r * LR, 1, qx);
+          const int r = r0 + lsub;
+          if (lact && r < NZR * LR)
+            s1[r * LQ + lq] = reduce1(sf + r * LR, 1, lq);
         }
       __syncthreads();
-      for (int i = threadIdx.x; i < NZR * LQ * LQ; i += blockDim.x)
+      // y: s1[z][fy][qx] -> s2[z][qy][qx]
+      for (int r0 = warp * GQ; r0 < NZR * LQ; r0 += NW * GQ)
         {
-          const int qx = i % LQ, qy = (i / LQ) % LQ, z = i / (LQ * LQ);
-          s2[i]        = reduce1(s1 + z * LR * LQ + qx, LQ, qy);
+          const int r = r0 + lsub;
+          if (lact && r < NZR * LQ)
+            {
+              const int z = r / LQ, qy = r - z * LQ;
+              s2[r * LQ + lq] = reduce1(s1 + z * LR * LQ + lq, LQ, qy);
+            }
         }
       __syncthreads();
-      batched_add<4>(NZQ * LQ * LQ, dst, [&](int i, long long &off, T &v) {
-        const int qx = i % LQ, qy = (i / LQ) % LQ, qz = i / (LQ * LQ);
-        const int g[3] = {q0[0] + qx, q0[1] + qy, DIM == 3 ? q0[2] + qz : 0};
-        bool own = (qx < LQ - 1 || g[0] == cm.nn[0] - 1) && (qy < LQ - 1 || g[1] == cm.nn[1] - 1);
-        if (DIM == 3)
-          own = own && (qz < LQ - 1 || g[2] == cm.nn[2] - 1);
-        own = own && g[0] < cm.nn[0] && g[1] < cm.nn[1] && (DIM < 3 || g[2] < cm.nn[2]);
-        if (!own || is_boundary_node(cm, g[0], g[1], g[2]))
-          return false;
-        v   = DIM == 3 ? reduce1(s2 + qy * LQ + qx, LQ * LQ, qz) : s2[i];
-        off = j * cm.N + g[0] + (long long)cm.nn[0] * (g[1] + (long long)cm.nn[1] * g[2]);
-        return true;
-      });
+      // z (3-D) and the owned coarse nodes added to dst: rows (qz, qy) GQ
+      // per warp step, all of a lane's dst loads in flight before its stores
+      constexpr int NRQ = NZQ * LQ;
+      constexpr int KB  = (NRQ + NW * GQ - 1) / (NW * GQ);
+      const int     g0  = q0[0] + lq;
+      const bool    ownx = lq < LQ - 1 || g0 == cm.nn[0] - 1;
+      const bool    inx  = g0 > 0 && g0 < cm.nn[0] - 1;
+      long long     off[KB];
+      T             v[KB], old[KB];
+      bool          ok[KB];
+#pragma unroll
+      for (int kb = 0; kb < KB; ++kb)
+        {
+          const int r = warp * GQ + kb * NW * GQ + lsub;
+          ok[kb]      = false;
+          if (!lact || r >= NRQ || !ownx || !inx)
+            continue;
+          const int qz = DIM == 3 ? r / LQ : 0, qy = r - qz * LQ;
+          const int g1 = q0[1] + qy, g2 = DIM == 3 ? q0[2] + qz : 0;
+          bool      own = (qy < LQ - 1 || g1 == cm.nn[1] - 1) && g1 > 0 && g1 < cm.nn[1] - 1;
+          if (DIM == 3)
+            own = own && (qz < LQ - 1 || g2 == cm.nn[2] - 1) && g2 > 0 && g2 < cm.nn[2] - 1;
+          if (!own)
+            continue;
+          v[kb]   = DIM == 3 ? reduce1(s2 + qy * LQ + lq, LQ * LQ, qz) : s2[r * LQ + lq];
+          off[kb] = j * cm.N + g0 + (long long)cm.nn[0] * (g1 + (long long)cm.nn[1] * g2);
+          ok[kb]  = true;
+        }
+#pragma unroll
+      for (int kb = 0; kb < KB; ++kb)
+        old[kb] = ok[kb] ? dst[off[kb]] : T(0);
+#pragma unroll
+      for (int kb = 0; kb < KB; ++kb)
+        if (ok[kb])
+          dst[off[kb]] = old[kb] + v[kb];
     }
 
     template <int DIM, int P, typename T>
