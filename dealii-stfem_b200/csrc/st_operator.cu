@@ -112,10 +112,11 @@ namespace stmg
 
   // Tile shape of an operator apply on mesh m with elements of elem bytes:
   // the big shape unless it does not fit in shared memory, or it yields
-  // fewer than two tiles per SM while the small shape still gives each CTA
-  // several cells (a one-cell tile keeps only nt_out threads of a CTA busy
-  // in phase B, far slower than a partly filled GPU of big tiles). Used by
-  // StOperator and by the allocation-free box apply, so both pick the same.
+  // fewer than two tiles per SM (in 3-D: than half a tile per SM) while the
+  // small shape still gives each CTA several cells (a one-cell tile keeps
+  // only nt_out threads of a CTA busy in phase B, far slower than a partly
+  // filled GPU of big tiles). Used by StOperator and by the allocation-free
+  // box apply, so both pick the same.
   Tiling
   choose_op_tiling(const MeshView &m, std::size_t elem, int nt_in_, int nt_out_, bool &big_out, int *shape)
   {
@@ -132,7 +133,11 @@ namespace stmg
         shp(big, T3);
         if (op_smem_bytes(m.dim, m.p, T3, nt_in_, nt_out_, elem) <= budget)
           {
-            if (big && make_tiling(m, T3).n_tiles < 2ll * sm_count())
+            // 3-D: the big shape down to half a tile per SM (32^3 Q2: 128 big
+            // tiles in one round, 37 us, against 1,024 small ones in 3.5
+            // rounds, 57 us; at 16^3, 16 big tiles lose to 128 small ones)
+            const long long few = m.dim == 3 ? sm_count() / 2 : 2ll * sm_count();
+            if (big && make_tiling(m, T3).n_tiles < few)
               {
                 int t3[3];
                 shp(false, t3);
