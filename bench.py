@@ -643,8 +643,8 @@ def main():
                     help="skip the per-slab comparison of the FP32-MG and FP64-MG solutions with a converged "
                          "FP64 solve")
     ap.add_argument("--kernels-only", choices=["all", "st_apply", "st_apply64", "vanka_apply", "h_transfer"], default=None,
-                    help="only time the finest-level operator (FP32 or FP64) and/or Vanka apply in isolation "
-                         "(profiling)")
+                    help="only time the finest-level operator (FP32 or FP64), Vanka apply and/or h-transfers "
+                         "in isolation (profiling)")
     ap.add_argument("--adjoint", action="store_true", help="time the adjoint gradient configuration")
     ap.add_argument("--config", choices=["c1", "c2", "c3"], default=None,
                     help="time one of the other configurations (not the main metric line)")
