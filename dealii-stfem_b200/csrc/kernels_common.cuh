@@ -36,6 +36,68 @@ namespace stmg
         v += rhs[i];
       dst[i] = v;
     }
+    // dst[i + k stride] for k < n (n <= K), each as write() computes it,
+    // with every load of dst and rhs issued before the first store (the
+    // time blocks of a node would otherwise be n dependent round trips:
+    // nothing tells the compiler the addresses differ)
+    template <int K>
+    __device__ __forceinline__ void
+    write_n(T *dst, long long i, long long stride, const T (&s)[K], int n = K) const
+    {
+      T d[K], r[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        {
+          d[k] = r[k] = T(0);
+          if (k < n)
+            {
+              if (beta != T(0))
+                d[k] = dst[i + k * stride];
+              if (rhs)
+                r[k] = rhs[i + k * stride];
+            }
+        }
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (k < n)
+          {
+            T v = alpha * s[k];
+            if (beta != T(0))
+              v += beta * d[k];
+            if (rhs)
+              v += r[k];
+            dst[i + k * stride] = v;
+          }
+    }
+    template <int K>
+    __device__ __forceinline__ void
+    write_constrained_n(T *dst, long long i, long long stride, int n = K) const
+    {
+      T d[K], r[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        {
+          d[k] = r[k] = T(0);
+          if (k < n)
+            {
+              if (beta != T(0))
+                d[k] = dst[i + k * stride];
+              if (rhs)
+                r[k] = rhs[i + k * stride];
+            }
+        }
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (k < n)
+          {
+            T v = T(0);
+            if (beta != T(0))
+              v += beta * d[k];
+            if (rhs)
+              v += r[k];
+            dst[i + k * stride] = v;
+          }
+    }
   };
 
   template <int P1, int DIM>
@@ -359,8 +421,8 @@ namespace stmg
     const long long node = g[0] + (long long)n0 * (g[1] + (long long)n1 * g[2]);
     if (boundary)
       {
-        for (int j = 0; j < nt; ++j)
-          om.write_constrained(dst, j * m.N + node);
+        for (int j0 = 0; j0 < nt; j0 += 4)
+          om.template write_constrained_n<4>(dst, node + (long long)j0 * m.N, m.N, min(4, nt - j0));
         return;
       }
     if (is_boundary_node(m, g[0], g[1], g[2]))
@@ -417,10 +479,11 @@ namespace stmg
             for (int jj = 0; jj < 4; ++jj)
               if (j0 + jj < nt)
                 s[jj] += shell[off[c] + (long long)(j0 + jj) * tl.tile_stride];
+        T v[4];
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj)
-          if (j0 + jj < nt)
-            om.write(dst, node + (long long)(j0 + jj) * m.N, s[jj] * w);
+          v[jj] = s[jj] * w;
+        om.template write_n<4>(dst, node + (long long)j0 * m.N, m.N, v, min(4, nt - j0));
       }
   }
 

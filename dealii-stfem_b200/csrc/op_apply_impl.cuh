@@ -827,35 +827,46 @@ namespace stmg
                   const T   *cj    = c;
                   long long  gj    = grow + bx; // index into dst and rhs
                   T         *sj    = shell + (long long)tile * nto * tl.tile_stride + slot;
-                  for (int j = 0; j < nto; ++j, cj += ND, gj += m.N, sj += tl.tile_stride)
+                  // four time dofs at a time, their dst / rhs loads issued
+                  // before their stores (OutMode::write_n)
+                  for (int j0 = 0; j0 < nto; j0 += 4, gj += 4 * m.N)
                     {
-                      T s = cj[0];
-                      if (two)
-                        s += cj[dx];
-                      if (ty)
+                      const int cnt = min(4, nto - j0);
+                      T         sv[4];
+#pragma unroll
+                      for (int jj = 0; jj < 4; ++jj, cj += ND, sj += tl.tile_stride)
                         {
-                          s += cj[dy];
+                          if (jj >= cnt)
+                            break;
+                          T s = cj[0];
                           if (two)
-                            s += cj[dy + dx];
-                        }
-                      if (tz)
-                        {
-                          s += cj[dz];
-                          if (two)
-                            s += cj[dz + dx];
+                            s += cj[dx];
                           if (ty)
                             {
-                              s += cj[dz + dy];
+                              s += cj[dy];
                               if (two)
-                                s += cj[dz + dy + dx];
+                                s += cj[dy + dx];
                             }
+                          if (tz)
+                            {
+                              s += cj[dz];
+                              if (two)
+                                s += cj[dz + dx];
+                              if (ty)
+                                {
+                                  s += cj[dz + dy];
+                                  if (two)
+                                    s += cj[dz + dy + dx];
+                                }
+                            }
+                          sv[jj] = s;
+                          if (!inner && tl.n_tiles != 1)
+                            *sj = s;
                         }
                       if (inner)
-                        om.write(dst, gj, s);
+                        om.write_n(dst, gj, m.N, sv, cnt);
                       else if (tl.n_tiles == 1)
-                        om.write_constrained(dst, gj);
-                      else
-                        *sj = s;
+                        om.template write_constrained_n<4>(dst, gj, m.N, cnt);
                     }
                 }
             }

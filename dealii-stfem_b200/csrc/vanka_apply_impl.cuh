@@ -664,15 +664,16 @@ namespace stmg
                   const float w = v == 1 ? 1.0f : (v == 2 ? 0.5f : (v == 4 ? 0.25f : 0.125f));
                   float       o[NT];
                   TV::load(bout + ((bz * S::E1 + by) * S::E0 + lx) * NTP, o);
-                  long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+                  const long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
                   if (inte)
+                    {
 #pragma unroll
-                    for (int j = 0; j < NT; ++j, gi += m.N)
-                      om.write(dst, gi, o[j] * w);
+                      for (int j = 0; j < NT; ++j)
+                        o[j] *= w;
+                      om.write_n(dst, gi, m.N, o);
+                    }
                   else if (tl.n_tiles == 1)
-#pragma unroll
-                    for (int j = 0; j < NT; ++j, gi += m.N)
-                      om.write_constrained(dst, gi);
+                    om.template write_constrained_n<NT>(dst, gi, m.N);
                   else
                     {
                       float *sj = shell + (long long)tile * NT * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz);
@@ -907,15 +908,16 @@ namespace stmg
           float       o[NT];
           TV::load(bout + ((bz * S::E1 + by) * S::E0 + lx) * NTP, o);
           time_map<NT>(te.S, o);
-          long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+          const long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
           if (inte)
+            {
 #pragma unroll
-            for (int jt = 0; jt < NT; ++jt, gi += m.N)
-              om.write(dst, gi, o[jt] * w);
+              for (int jt = 0; jt < NT; ++jt)
+                o[jt] *= w;
+              om.write_n(dst, gi, m.N, o);
+            }
           else if (tl.n_tiles == 1)
-#pragma unroll
-            for (int jt = 0; jt < NT; ++jt, gi += m.N)
-              om.write_constrained(dst, gi);
+            om.template write_constrained_n<NT>(dst, gi, m.N);
           else
             {
               float *sj = shell + (long long)tile * NT * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz);
@@ -1800,15 +1802,16 @@ namespace stmg
                   float       ov[NT];
                   TV::load(bout + ((bz * S::E1 + by) * S::E0 + lx) * NTP, ov);
                   time_map<NT>(te.S, ov);
-                  long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
+                  const long long gi = gx + (long long)m.nn[0] * (gy + (long long)m.nn[1] * gz);
                   if (inte)
+                    {
 #pragma unroll
-                    for (int jt = 0; jt < NT; ++jt, gi += m.N)
-                      om.write(dst, gi, ov[jt] * w);
+                      for (int jt = 0; jt < NT; ++jt)
+                        ov[jt] *= w;
+                      om.write_n(dst, gi, m.N, ov);
+                    }
                   else if (tl.n_tiles == 1)
-#pragma unroll
-                    for (int jt = 0; jt < NT; ++jt, gi += m.N)
-                      om.write_constrained(dst, gi);
+                    om.template write_constrained_n<NT>(dst, gi, m.N);
                   else
                     {
                       float *sj = shell + (long long)tile * NT * tl.tile_stride + shell_slot<DIM>(tl, tg.e, lx, by, bz);
