@@ -48,7 +48,9 @@ def parse_tp01(text):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/extract_golden.py /path/to/reference")
+    ref = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(ref, "tests", "tp_01.output")) as f:
         rows = parse_tp01(f.read())
